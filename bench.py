@@ -1,0 +1,406 @@
+"""Benchmark: site-updates/s of the fused FP32 KDK step at 3D 512^3 on B200.
+
+Workload (the 512^3 configuration): periodic box L = 1, psi = sqrt(1+delta)
+with delta a Gaussian random field (P(k) ~ k^-2 exp(-(k/kc)^2), kc = N/8 * 2pi,
+sigma 0.3, clipped at -0.9) plus 32 Schive-profile solitons (rc ~ U[0.01,
+0.03)), mean |psi|^2 = 1, pref = 4 pi G = 1, dt = 0.2 dx^2.  Synthetic data,
+seeded (Philox4x32-10), generated on the device in FP64.
+
+A "step" is one merged kick-drift-kick step (Field::drift_update +
+Field::full_kick of the reference's time loop) through qx_step: eight fused
+HBM passes over the 1 GiB complex64 state (inputs larger than L2 -- no
+flush needed).  The plain FP64 form (complex128) is measured the same way and
+reported beside it.  Only one box per GPU: a single box does not shard, so N > 1
+runs N independent replicas ("weak" scaling, no collective on the data path).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 512
+DIM = 3
+N_SOL = 32
+SEED = 1234
+METRIC = "site-updates/s @512^3 (fused FP32 KDK step, 1 B200)"
+UNIT = "site-updates/s"
+# algorithmic HBM bytes per site of one fused loop-body pass, w = bytes/real
+PASS_BYTES_W = {
+    "y_fwd(psi)": 4, "z_drift(psi)": 4, "y_inv(psi)": 4, "x_inv_r2c(psi->rho^)": 5,
+    "y_fwd(rho^)": 2, "z_poisson(rho^)": 2, "y_inv(rho^)": 2, "x_c2r_kick_fwd": 5,
+}
+ROOFLINE_BYTES_W = 26  # graded per-site minimum of the whole step (26 w)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier_sync(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_field(qx, dtype, dt):
+    f = qx.Field(DIM, N_GRID, L=1.0, pref=1.0, rho_mean=1.0, dtype=dtype, k0="zero" if dtype == "c64" else "reference",
+                 dt=dt)
+    f.ic_config(qx.IC_GRF, SEED, N_SOL, 0.01, 0.03)
+    return f
+
+
+def time_form(qx, dtype, dt, K, W, world, device, sample_clocks=False):
+    f = make_field(qx, dtype, dt)
+    f.step(W)                     # warm-up (also captures the loop-body graph)
+    barrier_sync(world)
+    clocks = None
+    if sample_clocks:
+        with ClockSampler(device) as cs:
+            ms = f.time_steps(K, True)
+        clocks = cs.summary()
+    else:
+        ms = f.time_steps(K, True)
+    barrier_sync(world)
+    ms = max_over_ranks(ms, world)
+    return f, ms, clocks
+
+
+def cpu_baseline(psi0, dt, budget_s=20.0):
+    """The reference's own CPU path (oracle/_ref: its field/spectrum/IC sources
+    + project FFTW shim, OpenMP on every host core): loop-body steps
+    (Field::drift_update + Field::full_kick) of the same 512^3 state."""
+    from oracle import ref_lib as R
+    if not R.available():
+        return None
+    cores = os.cpu_count()
+    f = R.RefField(DIM, N_GRID, 1.0, 1.0 / (4.0 * math.pi), dt, cores)
+    f.set_psi(psi0)
+    f.update_potential()
+    f.half_kick()
+    n, t = 0, 0.0
+    while n < 1 or (t < budget_s and n < 3):
+        t0 = time.perf_counter()
+        f.loop_body(1)
+        t += time.perf_counter() - t0
+        n += 1
+    f.close()
+    S = N_GRID ** DIM
+    return {"value": S * n / t, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{n} KDK loop-body step(s) of the 512^3 state (complex128, reference loops + project FFTW shim)",
+            "s_per_step": t / n}
+
+
+def run_reference_arm(args, world, rank):
+    """--impl reference: the reference's CPU implementation of the path on the
+    host cores (oracle/_ref built from its sources)."""
+    if rank != 0:
+        return
+    from oracle import ref_lib as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libqx_ref.so missing"}))
+        return
+    from oracle import sp_oracle as O
+    cores = os.cpu_count()
+    N = N_GRID
+    dt = 0.2 / N**2
+    # same workload; the IC is built with the oracle's FP64 generator at 512^3
+    # would take minutes in NumPy, so the box state is a smooth GRF-like field
+    # of the same size (the step's cost does not depend on the values)
+    rng = np.random.default_rng(SEED)
+    psi = (1.0 + 0.05 * rng.standard_normal((N,) * DIM)).astype(np.complex128)
+    psi = O.normalise_mean_density(psi)
+    f = R.RefField(DIM, N, 1.0, 1.0 / (4.0 * math.pi), dt, cores)
+    f.set_psi(psi)
+    del psi
+    f.update_potential()
+    f.half_kick()
+    t0 = time.perf_counter()
+    f.loop_body(1)
+    t_one = time.perf_counter() - t0
+    sample_n = N
+    total = t_one * (args.steps + args.warmup)
+    if total > 240.0:  # keep the arm within a few minutes: one 256^3 box per step
+        f.close()
+        sample_n = 256
+        f = R.RefField(DIM, sample_n, 1.0, 1.0 / (4.0 * math.pi), 0.2 / sample_n**2, cores)
+        f.set_psi(np.ones((sample_n,) * DIM, np.complex128))
+        f.update_potential()
+        f.half_kick()
+    for _ in range(max(0, args.warmup - 1)):
+        f.loop_body(1)
+    t0 = time.perf_counter()
+    f.loop_body(args.steps)
+    t = time.perf_counter() - t0
+    f.close()
+    S = sample_n ** DIM
+    value = S * args.steps / t
+    sample = f"one KDK loop-body step of a {sample_n}^3 complex128 box per step"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3D 512^3 Schroedinger-Poisson KDK step", "grid": N_GRID, "dim": DIM,
+                   "sample_grid": sample_n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def e2e_run(qx, dt, K, host_in, host_out, world):
+    """Through the C ABI with pinned host buffers: upload psi0, K steps,
+    download psi (the copies are inside the timed region)."""
+    f = qx.Field(DIM, N_GRID, L=1.0, pref=1.0, dtype="c64", k0="zero", dt=dt)
+    f.set_psi_ptr(host_in)
+    f.step(2)
+    barrier_sync(world)
+    t0 = time.perf_counter()
+    f.set_psi_ptr(host_in)
+    f.step(K)
+    f.get_psi_ptr(host_out)
+    t = time.perf_counter() - t0
+    barrier_sync(world)
+    f.close()
+    return max_over_ranks(t, world)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--accuracy-steps", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+
+    import qaxions_b200 as qx
+    qx.set_device(local)
+    K, W = args.steps, args.warmup
+    S = N_GRID ** DIM
+    dt = 0.2 / N_GRID**2
+    hbm, peak_kind = peaks()
+
+    # ---- fused FP32 form (the headline) ----
+    f32, ms32, clocks = time_form(qx, "c64", dt, K, W, world, local, sample_clocks=True)
+    prof = f32.profile_step(max(3, min(K, 10)))
+    f32.close()
+    # ---- plain FP64 form ----
+    f64, ms64, _ = time_form(qx, "c128", dt, K, W, world, local)
+    f64.close()
+
+    value = world * S * K / (ms32 / 1e3)
+    value64 = world * S * K / (ms64 / 1e3)
+    ms_step = ms32 / K
+
+    # ---- roofline of the dominant pass ----
+    w = 4
+    top = max(prof, key=lambda p: p[1])
+    per_pass = []
+    for name, t in prof:
+        b = PASS_BYTES_W.get(name, 0) * w * S
+        per_pass.append({"pass": name, "us": 1e3 * t, "alg_bytes": b, "gbs": b / (t * 1e-3) / 1e9})
+    top_b = PASS_BYTES_W[top[0]] * w * S
+    achieved = top_b / (top[1] * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic_512.txt")
+    if os.path.exists(tfile):
+        for line in open(tfile):
+            p = line.split()
+            if len(p) >= 2 and p[0] == top[0]:
+                traffic = float(p[1])
+    step_bytes = sum(PASS_BYTES_W.values()) * w * S
+    roofline = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                "alg_bytes_per_launch": top_b, "launch_us": 1e3 * top[1], "per_pass": per_pass,
+                "step_alg_bytes": step_bytes, "step_gbs": step_bytes / (ms_step * 1e-3) / 1e9,
+                "graded_roofline_26w": {
+                    "bytes_per_site": ROOFLINE_BYTES_W * w,
+                    "frac_of_8TBs": ROOFLINE_BYTES_W * w * S / (ms_step * 1e-3) / 8e12,
+                    "frac_of_measured": ROOFLINE_BYTES_W * w * S / (ms_step * 1e-3) / (hbm * 1e9)}}
+
+    # ---- accuracy after --accuracy-steps (FP32 vs FP64 plain form, same IC) ----
+    acc = None
+    if rank == 0 and args.accuracy_steps > 0:
+        a = make_field(qx, "c128", dt)
+        b = make_field(qx, "c64", dt)
+        M0, E0, _, _ = a.mass_energy()
+        a.step(args.accuracy_steps)
+        b.step(args.accuracy_steps)
+        pa, pb = a.psi, b.psi
+        Va, Vb = a.V, b.V
+        Ma, Ea, _, _ = a.mass_energy()
+        Mb, Eb, _, _ = b.mass_energy()
+        ka, Pa, ca = a.spectrum(0, qx.SPEC_LOG, 256)
+        kb, Pb, cb = b.spectrum(0, qx.SPEC_LOG, 256)
+        sel = ca > 0
+        acc = {"steps": args.accuracy_steps,
+               "relL2_psi_fp32_vs_fp64": float(np.linalg.norm(pb - pa) / np.linalg.norm(pa)),
+               "relL2_V_fp32_vs_fp64": float(np.linalg.norm((Vb - Vb.mean()) - (Va - Va.mean()))
+                                             / np.linalg.norm(Va - Va.mean())),
+               "mass_drift_fp64": abs(Ma - M0) / M0, "mass_drift_fp32": abs(Mb - M0) / M0,
+               "energy_drift_fp64": abs(Ea - E0) / abs(E0), "energy_drift_fp32": abs(Eb - E0) / abs(E0),
+               "Pk_log256_max_rel_err": float(np.max(np.abs(Pb[sel] - Pa[sel]) / np.abs(Pa[sel]))),
+               "reference_form": "plain FP64 GPU form (validated against the CPU oracle at <=1e-12)"}
+        del pa, pb, Va, Vb
+        a.close()
+        b.close()
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        g = make_field(qx, "c128", dt)
+        psi0 = g.psi
+        g.close()
+        cpu = cpu_baseline(psi0, dt)
+        del psi0
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    host_in = torch.empty(2 * S, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(2 * S, dtype=torch.float64, pin_memory=True)
+    g = make_field(qx, "c64", dt)
+    g.get_psi_ptr(host_in.data_ptr())
+    g.close()
+    t_e2e = e2e_run(qx, dt, K, host_in.data_ptr(), host_out.data_ptr(), world)
+    e2e = {"value": world * S * K / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 16 * S / K,
+           "d2h_bytes_per_step": 16 * S / K,
+           "what": f"qx_set_psi (FP64 pinned host -> device) + qx_step({K}) + qx_get_psi (device -> pinned host)"}
+    del host_in, host_out
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 (fp32 complex; fp64 phase args, reductions, spectrum sums)", "data": "synthetic",
+            "config": {"workload": "3D 512^3 GRF + 32 Schive solitons, merged KDK step (fused FP32 form)",
+                       "grid": N_GRID, "dim": DIM, "dt": dt, "pref": 1.0, "seed": SEED,
+                       "l2": "inputs larger than L2 (1 GiB complex64 state per pass)",
+                       "parallelism": f"replicas x{world} (one box per GPU)"},
+            "plain_fp64": {"value": value64, "ms_per_step": ms64 / K, "dtype": "c128"},
+            "fp32_over_fp64": value / value64,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 5 + 8 * K,
+            "clocks": clocks,
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+/*
+ * qaxions_b200.h -- C ABI of the B200-native Schroedinger-Poisson solver core.
+ *
+ * One opaque handle per periodic 2D/3D box.  Every entry point returns an int
+ * status (QX_OK = 0); on failure qx_last_error(handle) gives the message
+ * (qx_last_error(NULL) for failures of qx_create).  No C++ exception crosses
+ * this boundary.  Host arrays are FP64 in the reference's memory order
+ * (3D: idx = iz*N*N + iy*N + ix, x fastest; complex interleaved re,im), whatever
+ * the device precision.  A handle owns its device buffers and one CUDA stream;
+ * it is not thread-safe.
+ *
+ * Each declaration names the reference interface it replaces
+ * (gpierobon/qaxions, path:line).
+ */
+#ifndef QAXIONS_B200_H
+#define QAXIONS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QX_OK 0
+#define QX_ERR_INVALID 1     /* bad argument / unsupported shape        */
+#define QX_ERR_CUDA 2        /* CUDA runtime or launch failure          */
+#define QX_ERR_NOMEM 3       /* device allocation failed                */
+#define QX_ERR_STATE 4       /* call not valid in the handle's state    */
+#define QX_ERR_INTERNAL 5
+
+#define QX_C128 0            /* plain FP64 form (complex128)            */
+#define QX_C64 1             /* fused FP32 form (complex64)             */
+
+#define QX_K0_REFERENCE 0    /* k=0 Poisson mode divided by 1 (src/field.cxx:253,282) */
+#define QX_K0_ZERO 1         /* k=0 Poisson mode set to exactly 0       */
+
+#define QX_SPEC_REFERENCE 0  /* integer shells round(|n|), N/2+1 bins (src/spectrum/spectrum.cxx:63-155) */
+#define QX_SPEC_LINEAR 1     /* nbins linear bins over 0 < |n| < N/2    */
+#define QX_SPEC_LOG 2        /* nbins log bins over 1 <= |n| < N/2      */
+
+#define QX_IC_SOLITONS 0     /* sum of Schive-profile solitons          */
+#define QX_IC_GRF 1          /* sqrt(1 + delta), delta a Gaussian random field (+ solitons if n > 0) */
+
+typedef struct qx_field_s qx_field_t;
+
+int qx_version(void);
+const char *qx_last_error(const qx_field_t *h);
+/* select the CUDA device for handles created afterwards by this thread
+ * (one process per GPU: the reference's --nthr thread setting,
+ * src/parse.cxx:162, has no GPU counterpart; this is its placement knob) */
+int qx_set_device(int device);
+
+/* Field construction: Field::Field(Params&) / Field::init / setCosmo
+ * (src/field.cxx:13-46,68-91), STATIC cosmology.  pref = norm_*a_
+ * (src/field.cxx:78,298), rho_mean = rho_mean_ (src/field.cxx:77),
+ * dt = ds_ (src/field.cxx:77).  Supported N: 4, 8, 16, 32, 64, 96, 128, 256, 512. */
+int qx_create(int dim, int N, double L, double pref, double rho_mean, int dtype, int k0_policy,
+              double dt, qx_field_t **out);
+/* Field::~Field (src/field.cxx:58-66) */
+int qx_destroy(qx_field_t *h);
+/* ds_ (src/field.h:82) */
+int qx_set_dt(qx_field_t *h, double dt);
+
+/* Field::psi() / getPsiIdx / getPsiImagIdx (src/field.h:36-39): 2*sites doubles */
+int qx_set_psi(qx_field_t *h, const double *psi);
+int qx_get_psi(qx_field_t *h, double *psi);
+/* Field::V() / getVIdx (src/field.h:41-43): sites doubles */
+int qx_set_V(qx_field_t *h, const double *V);
+int qx_get_V(qx_field_t *h, double *V);
+/* Field::Vhat() (src/field.h:45): 2*ksites doubles in FFTW r2c layout
+ * [..][N/2+1] (the device keeps a packed N/2-column form) */
+int qx_get_Vhat(qx_field_t *h, double *vhat);
+int qx_set_Vhat(qx_field_t *h, const double *vhat);
+
+/* Field::kick (src/field.cxx:93-116) */
+int qx_kick(qx_field_t *h, double dt);
+/* Field::drift (src/field.cxx:119-198) */
+int qx_drift(qx_field_t *h, double dt);
+/* Field::Poisson (src/field.cxx:230-291), on the transformed V^ */
+int qx_poisson(qx_field_t *h);
+/* Field::updatePotential (src/field.cxx:294-346) */
+int qx_update_potential(qx_field_t *h);
+/* Field::computeEnergy (src/field.cxx:200-227): V <- |psi|^2, rhomax */
+int qx_compute_energy(qx_field_t *h);
+/* Field::updateTime / half_kick / full_kick / drift_update / propagate
+ * (src/field.cxx:349-402) */
+int qx_update_time(qx_field_t *h);
+int qx_half_kick(qx_field_t *h);
+int qx_full_kick(qx_field_t *h);
+int qx_drift_update(qx_field_t *h);
+int qx_propagate(qx_field_t *h);
+/* The KDK time loop of main() (src/main.cxx:64-85) with measurements off:
+ * updatePotential, half_kick, nsteps x (drift_update, full_kick but the last),
+ * half_kick -- fused passes, loop body replayed from a CUDA graph. */
+int qx_step(qx_field_t *h, int nsteps);
+
+/* Field::Vmax / rhomax / time / a / curr (src/field.h:56-62) */
+int qx_scalars(qx_field_t *h, double *vmax, double *rhomax, double *time, double *a, int *curr);
+/* computeEnergy's rhomax and updatePotential's Vmax without overwriting V
+ * (src/field.cxx:216-226,338-345) */
+int qx_rho_stats(qx_field_t *h, double *rhomax, double *vmax);
+/* mass and energy diagnostics (no reference counterpart; M = sum |psi|^2 dV,
+ * E = K + W, K spectral, W = 1/2 sum V |psi|^2 dV) */
+int qx_mass_energy(qx_field_t *h, double *M, double *E, double *K, double *W);
+/* Spectrum::compute + Pk/counts/kmodes (src/spectrum/spectrum.cxx:32-164,
+ * src/spectrum/spectrum.h:21-32).  source 0: |psi|^2 (what measure() bins
+ * after computeEnergy, src/meas.cxx:30-41), 1: V.  Arrays hold nbins entries
+ * (N/2+1 for QX_SPEC_REFERENCE, nbins ignored). */
+int qx_spectrum(qx_field_t *h, int source, int mode, int nbins, double *k, double *P, long long *count);
+
+/* FFTBackend::forward_c2c / backward_c2c / forward_r2c / backward_c2r
+ * (src/fft/fft.h:14-17) on host buffers; sign -1 forward, +1 backward;
+ * r2c/c2r halves use FFTW's [..][N/2+1] layout; all unnormalised. */
+int qx_fft_c2c(qx_field_t *h, double *data, int sign);
+int qx_fft_r2c(qx_field_t *h, const double *in, double *out);
+int qx_fft_c2r(qx_field_t *h, const double *in, double *out);
+
+/* SolitonsIC::apply (src/ic/solitons.cxx:20-110): Gaussian 'solitons' from a
+ * solitons.txt-format file (rows: amp sigma x y z) over background bkg. */
+int qx_ic_solitons_file(qx_field_t *h, const char *path, double bkg);
+/* the same from an in-memory table of n rows {amp, sigma, x, y, z} */
+int qx_ic_gaussian_solitons(qx_field_t *h, int n, const double *rows5, double bkg);
+/* synthetic benchmark initial conditions (no reference counterpart):
+ * kind QX_IC_SOLITONS (psi = sum of n Schive solitons) or QX_IC_GRF
+ * (psi = sqrt(1+delta) + n solitons), delta ~ P(k) = k^-2 exp(-(k/kc)^2),
+ * kc = kc_factor*N*2pi/L, std sigma, clipped at clip; soliton rc ~ U[rc_lo,
+ * rc_hi), rho_c = rho0 rc^-4, centres ~ U[0,1)^d, phases ~ U[0,2pi) from
+ * Philox4x32-10 keyed by seed; finally mean |psi|^2 = 1. */
+int qx_ic_config(qx_field_t *h, int kind, unsigned long long seed, int n_solitons, double rc_lo,
+                 double rc_hi, double sigma, double kc_factor, double clip, double rho0);
+
+/* device time (CUDA events on the handle's stream) of qx_step(nsteps) */
+int qx_time_steps(qx_field_t *h, int nsteps, int use_graph, float *ms);
+/* per-pass average device time of the fused loop body over nsteps bodies;
+ * names: max_entries x 64 chars.  Advances the state. */
+int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, double *ms, int *n_out);
+/* launch geometry overrides (0 = default) */
+int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx);
+int qx_device_pointers(qx_field_t *h, void **psi, void **V);
+int qx_sync(qx_field_t *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

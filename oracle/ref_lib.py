@@ -1,0 +1,126 @@
+"""ctypes loader for oracle/_ref/libqx_ref.so -- the reference solver's own
+translation units built against the project FFTW shim (oracle/Makefile).
+
+TEST INFRASTRUCTURE (oracle and timed CPU baseline only).  ``available()`` is
+False when the library was not built (it is built from the reference sources,
+which exist only where those sources are present).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libqx_ref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        vp, d, i, dp, ip = C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)
+        sig = {
+            "ref_create": ([i, i, d, d, d, i], vp),
+            "ref_destroy": ([vp], None),
+            "ref_sites": ([vp], C.c_size_t),
+            "ref_ksites": ([vp], C.c_size_t),
+            "ref_set_psi": ([vp, dp], None),
+            "ref_get_psi": ([vp, dp], None),
+            "ref_set_V": ([vp, dp], None),
+            "ref_get_V": ([vp, dp], None),
+            "ref_get_Vhat": ([vp, dp], None),
+            "ref_ic_solitons": ([vp, d], None),
+            "ref_kick": ([vp, d], None),
+            "ref_drift": ([vp, d], None),
+            "ref_update_potential": ([vp], None),
+            "ref_poisson": ([vp], None),
+            "ref_compute_energy": ([vp], None),
+            "ref_half_kick": ([vp], None),
+            "ref_full_kick": ([vp], None),
+            "ref_drift_update": ([vp], None),
+            "ref_propagate": ([vp], None),
+            "ref_vmax": ([vp], d),
+            "ref_rhomax": ([vp], d),
+            "ref_time": ([vp], d),
+            "ref_curr": ([vp], i),
+            "ref_run": ([vp, i], None),
+            "ref_loop_body": ([vp, i], None),
+            "ref_spectrum": ([vp, dp, ip, dp], None),
+            "ref_fft_forward_c2c": ([vp, dp], None),
+            "ref_fft_backward_c2c": ([vp, dp], None),
+            "ref_fft_forward_r2c": ([vp, dp, dp], None),
+            "ref_fft_backward_c2r": ([vp, dp, dp], None),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class RefField:
+    """The reference ``Field`` (src/field.h:13-97) behind plain pointers.
+
+    norm is the reference's --norm: pref = 4 pi norm (src/field.cxx:78)."""
+
+    def __init__(self, dim: int, N: int, L: float = 1.0, norm: float = 1.0, dt: float = 1e-4,
+                 nthr: int = 1):
+        self.dim, self.N = dim, N
+        self.shape = (N,) * dim
+        self.hshape = (N,) * (dim - 1) + (N // 2 + 1,)
+        self.h = lib().ref_create(dim, N, L, norm, dt, nthr)
+
+    def close(self):
+        if self.h:
+            lib().ref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_psi(self, psi: np.ndarray):
+        a = np.ascontiguousarray(psi, dtype=np.complex128)
+        lib().ref_set_psi(self.h, _dp(a.view(np.float64)))
+
+    def psi(self) -> np.ndarray:
+        a = np.empty(self.shape, np.complex128)
+        lib().ref_get_psi(self.h, _dp(a.view(np.float64)))
+        return a
+
+    def set_V(self, V: np.ndarray):
+        a = np.ascontiguousarray(V, dtype=np.float64)
+        lib().ref_set_V(self.h, _dp(a))
+
+    def V(self) -> np.ndarray:
+        a = np.empty(self.shape, np.float64)
+        lib().ref_get_V(self.h, _dp(a))
+        return a
+
+    def Vhat(self) -> np.ndarray:
+        a = np.empty(self.hshape, np.complex128)
+        lib().ref_get_Vhat(self.h, _dp(a.view(np.float64)))
+        return a
+
+    def spectrum(self):
+        nb = self.N // 2 + 1
+        P = np.empty(nb)
+        k = np.empty(nb)
+        c = np.empty(nb, np.int32)
+        lib().ref_spectrum(self.h, _dp(P), c.ctypes.data_as(C.POINTER(C.c_int)), _dp(k))
+        return k, P, c.astype(np.int64)
+
+    def __getattr__(self, name):
+        f = getattr(lib(), "ref_" + name)
+        return lambda *a: f(self.h, *a)

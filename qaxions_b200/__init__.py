@@ -1,0 +1,353 @@
+"""qaxions_b200 -- B200-native Schroedinger-Poisson solver core.
+
+Python face of the C ABI in include/qaxions_b200.h (libqaxions_b200.so, built
+in-tree for sm_100a).  ``Field`` mirrors the reference's operator surface
+(gpierobon/qaxions src/field.h:17-64): kick, drift, Poisson, updatePotential,
+computeEnergy, updateTime, half_kick, full_kick, drift_update, propagate, plus
+``step`` (the fused, graph-replayed KDK loop of src/main.cxx:64-85).
+
+There is no CPU fallback: importing this package raises if the library is
+missing, and constructing a Field raises if no CUDA device is usable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqaxions_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "qaxions_b200.h")
+
+QX_OK, QX_ERR_INVALID, QX_ERR_CUDA, QX_ERR_NOMEM, QX_ERR_STATE, QX_ERR_INTERNAL = range(6)
+QX_C128, QX_C64 = 0, 1
+QX_K0_REFERENCE, QX_K0_ZERO = 0, 1
+SPEC_REFERENCE, SPEC_LINEAR, SPEC_LOG = 0, 1, 2
+IC_SOLITONS, IC_GRF = 0, 1
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C qaxions_b200/csrc -j8` "
+        "(or __graft_entry__.build()); there is no CPU fallback")
+
+_lib = C.CDLL(LIB_PATH)
+_vp, _d, _i = C.c_void_p, C.c_double, C.c_int
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_llp = C.POINTER(C.c_longlong)
+_fp = C.POINTER(C.c_float)
+
+_SIGS = {
+    "qx_version": ([], _i),
+    "qx_last_error": ([_vp], C.c_char_p),
+    "qx_set_device": ([_i], _i),
+    "qx_create": ([_i, _i, _d, _d, _d, _i, _i, _d, C.POINTER(_vp)], _i),
+    "qx_destroy": ([_vp], _i),
+    "qx_set_dt": ([_vp, _d], _i),
+    "qx_set_psi": ([_vp, _dp], _i),
+    "qx_get_psi": ([_vp, _dp], _i),
+    "qx_set_V": ([_vp, _dp], _i),
+    "qx_get_V": ([_vp, _dp], _i),
+    "qx_get_Vhat": ([_vp, _dp], _i),
+    "qx_set_Vhat": ([_vp, _dp], _i),
+    "qx_kick": ([_vp, _d], _i),
+    "qx_drift": ([_vp, _d], _i),
+    "qx_poisson": ([_vp], _i),
+    "qx_update_potential": ([_vp], _i),
+    "qx_compute_energy": ([_vp], _i),
+    "qx_update_time": ([_vp], _i),
+    "qx_half_kick": ([_vp], _i),
+    "qx_full_kick": ([_vp], _i),
+    "qx_drift_update": ([_vp], _i),
+    "qx_propagate": ([_vp], _i),
+    "qx_step": ([_vp, _i], _i),
+    "qx_scalars": ([_vp, _dp, _dp, _dp, _dp, _ip], _i),
+    "qx_rho_stats": ([_vp, _dp, _dp], _i),
+    "qx_mass_energy": ([_vp, _dp, _dp, _dp, _dp], _i),
+    "qx_spectrum": ([_vp, _i, _i, _i, _dp, _dp, _llp], _i),
+    "qx_fft_c2c": ([_vp, _dp, _i], _i),
+    "qx_fft_r2c": ([_vp, _dp, _dp], _i),
+    "qx_fft_c2r": ([_vp, _dp, _dp], _i),
+    "qx_ic_solitons_file": ([_vp, C.c_char_p, _d], _i),
+    "qx_ic_gaussian_solitons": ([_vp, _i, _dp, _d], _i),
+    "qx_ic_config": ([_vp, _i, C.c_ulonglong, _i, _d, _d, _d, _d, _d, _d], _i),
+    "qx_time_steps": ([_vp, _i, _i, _fp], _i),
+    "qx_profile_step": ([_vp, _i, _i, C.c_char_p, _dp, _ip], _i),
+    "qx_set_tune": ([_vp, _i, _i, _i], _i),
+    "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
+    "qx_sync": ([_vp], _i),
+}
+for _name, (_args, _res) in _SIGS.items():
+    _f = getattr(_lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res
+
+
+def lib():
+    """The loaded ctypes library (C ABI of include/qaxions_b200.h)."""
+    return _lib
+
+
+class QxError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[qx status {status}] {msg}")
+        self.status = status
+
+
+def _check(status: int, h=None):
+    if status != QX_OK:
+        msg = (_lib.qx_last_error(h) or b"").decode(errors="replace")
+        if status == QX_ERR_INVALID:
+            raise ValueError(msg)
+        if status == QX_ERR_NOMEM:
+            raise MemoryError(msg)
+        raise QxError(status, msg)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def set_device(device: int):
+    """Place fields created afterwards by this thread on CUDA device `device`."""
+    _check(_lib.qx_set_device(device))
+
+
+class Field:
+    """One periodic box (reference ``Field``, src/field.h:13-97).
+
+    dtype "c128" is the plain FP64 form, "c64" the fused FP32 form.  Host
+    arrays are complex128 / float64 in reference order ([z, y, x] / [y, x]).
+    ``pref`` is the Poisson prefactor (the reference's 4 pi norm a,
+    src/field.cxx:78,298)."""
+
+    def __init__(self, dim: int, N: int, L: float = 1.0, pref: float = 1.0, rho_mean: float = 1.0,
+                 dtype: str = "c128", k0: str = "reference", dt: float = 1e-4):
+        if dtype not in ("c128", "c64"):
+            raise ValueError("dtype must be 'c128' or 'c64'")
+        if k0 not in ("reference", "zero"):
+            raise ValueError("k0 must be 'reference' or 'zero'")
+        self._h = _vp()
+        _check(_lib.qx_create(dim, N, L, pref, rho_mean, QX_C128 if dtype == "c128" else QX_C64,
+                              QX_K0_REFERENCE if k0 == "reference" else QX_K0_ZERO, dt, C.byref(self._h)))
+        self.N_, self.dim_, self.L, self.dtype = N, dim, L, dtype
+        self.shape = (N,) * dim
+        self.hshape = (N,) * (dim - 1) + (N // 2 + 1,)
+
+    # -- lifetime --
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.qx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, name, *args):
+        _check(getattr(_lib, name)(self._h, *args), self._h)
+
+    # -- reference operator surface --
+    def kick(self, dt: float):
+        self._c("qx_kick", dt)
+
+    def drift(self, dt: float):
+        self._c("qx_drift", dt)
+
+    def Poisson(self):
+        self._c("qx_poisson")
+
+    def updatePotential(self):
+        self._c("qx_update_potential")
+
+    def computeEnergy(self):
+        self._c("qx_compute_energy")
+
+    def updateTime(self):
+        self._c("qx_update_time")
+
+    def half_kick(self):
+        self._c("qx_half_kick")
+
+    def full_kick(self):
+        self._c("qx_full_kick")
+
+    def drift_update(self):
+        self._c("qx_drift_update")
+
+    def propagate(self):
+        self._c("qx_propagate")
+
+    def step(self, nsteps: int):
+        self._c("qx_step", nsteps)
+
+    def set_dt(self, dt: float):
+        self._c("qx_set_dt", dt)
+
+    # -- buffers --
+    @property
+    def psi(self) -> np.ndarray:
+        a = np.empty(self.shape, np.complex128)
+        self._c("qx_get_psi", _ptr(a.view(np.float64)))
+        return a
+
+    @psi.setter
+    def psi(self, value):
+        a = np.ascontiguousarray(value, dtype=np.complex128).reshape(self.shape)
+        self._c("qx_set_psi", _ptr(a.view(np.float64)))
+
+    def set_psi_ptr(self, addr: int):
+        """Upload psi from a host buffer at `addr` (2*sites float64, e.g. pinned)."""
+        self._c("qx_set_psi", C.cast(C.c_void_p(addr), _dp))
+
+    def get_psi_ptr(self, addr: int):
+        """Download psi into a host buffer at `addr` (2*sites float64)."""
+        self._c("qx_get_psi", C.cast(C.c_void_p(addr), _dp))
+
+    @property
+    def V(self) -> np.ndarray:
+        a = np.empty(self.shape, np.float64)
+        self._c("qx_get_V", _ptr(a))
+        return a
+
+    @V.setter
+    def V(self, value):
+        a = np.ascontiguousarray(value, dtype=np.float64).reshape(self.shape)
+        self._c("qx_set_V", _ptr(a))
+
+    @property
+    def Vhat(self) -> np.ndarray:
+        a = np.empty(self.hshape, np.complex128)
+        self._c("qx_get_Vhat", _ptr(a.view(np.float64)))
+        return a
+
+    @Vhat.setter
+    def Vhat(self, value):
+        a = np.ascontiguousarray(value, dtype=np.complex128).reshape(self.hshape)
+        self._c("qx_set_Vhat", _ptr(a.view(np.float64)))
+
+    def getPsiIdx(self, idx: int) -> float:
+        return float(self.psi.ravel()[idx].real)
+
+    def getPsiImagIdx(self, idx: int) -> float:
+        return float(self.psi.ravel()[idx].imag)
+
+    def getVIdx(self, idx: int) -> float:
+        return float(self.V.ravel()[idx])
+
+    # -- scalars --
+    def _scalars(self):
+        v, r, t, a = (C.c_double() for _ in range(4))
+        c = C.c_int()
+        self._c("qx_scalars", C.byref(v), C.byref(r), C.byref(t), C.byref(a), C.byref(c))
+        return v.value, r.value, t.value, a.value, c.value
+
+    def size(self) -> int:
+        return self.N_
+
+    def dim(self) -> int:
+        return self.dim_
+
+    def sites(self) -> int:
+        return self.N_ ** self.dim_
+
+    def ksites(self) -> int:
+        return self.N_ ** (self.dim_ - 1) * (self.N_ // 2 + 1)
+
+    def Vmax(self) -> float:
+        return self._scalars()[0]
+
+    def rhomax(self) -> float:
+        return self._scalars()[1]
+
+    def time(self) -> float:
+        return self._scalars()[2]
+
+    def a(self) -> float:
+        return self._scalars()[3]
+
+    def curr(self) -> int:
+        return self._scalars()[4]
+
+    # -- measurements --
+    def rho_stats(self):
+        r, v = C.c_double(), C.c_double()
+        self._c("qx_rho_stats", C.byref(r), C.byref(v))
+        return r.value, v.value
+
+    def mass_energy(self):
+        """(M, E, K, W)."""
+        out = [C.c_double() for _ in range(4)]
+        self._c("qx_mass_energy", *(C.byref(o) for o in out))
+        return tuple(o.value for o in out)
+
+    def spectrum(self, source: int = 0, mode: int = SPEC_REFERENCE, nbins: int = 0):
+        """(k, P, count) shell-binned spectrum of |psi|^2 (source 0) or V (1)."""
+        nb = self.N_ // 2 + 1 if mode == SPEC_REFERENCE else nbins
+        k, P = np.empty(nb), np.empty(nb)
+        cnt = np.empty(nb, np.int64)
+        self._c("qx_spectrum", source, mode, nbins, _ptr(k), _ptr(P), cnt.ctypes.data_as(_llp))
+        return k, P, cnt
+
+    # -- FFT plugin on host buffers --
+    def fft_c2c(self, data: np.ndarray, sign: int) -> np.ndarray:
+        a = np.ascontiguousarray(data, dtype=np.complex128).reshape(self.shape).copy()
+        self._c("qx_fft_c2c", _ptr(a.view(np.float64)), sign)
+        return a
+
+    def fft_r2c(self, data: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(data, dtype=np.float64).reshape(self.shape)
+        out = np.empty(self.hshape, np.complex128)
+        self._c("qx_fft_r2c", _ptr(a), _ptr(out.view(np.float64)))
+        return out
+
+    def fft_c2r(self, data: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(data, dtype=np.complex128).reshape(self.hshape)
+        out = np.empty(self.shape, np.float64)
+        self._c("qx_fft_c2r", _ptr(a.view(np.float64)), _ptr(out))
+        return out
+
+    # -- initial conditions --
+    def ic_solitons_file(self, path: str = "solitons.txt", bkg: float = 1.0):
+        self._c("qx_ic_solitons_file", path.encode(), bkg)
+
+    def ic_gaussian_solitons(self, rows, bkg: float = 1.0):
+        a = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(-1, 5))
+        self._c("qx_ic_gaussian_solitons", a.shape[0], _ptr(a), bkg)
+
+    def ic_config(self, kind: int, seed: int, n_solitons: int = 0, rc_lo: float = 0.02, rc_hi: float = 0.05,
+                  sigma: float = 0.3, kc_factor: float = 0.125, clip: float = -0.9, rho0: float = 1.0e-6):
+        self._c("qx_ic_config", kind, seed, n_solitons, rc_lo, rc_hi, sigma, kc_factor, clip, rho0)
+
+    # -- timing --
+    def time_steps(self, nsteps: int, use_graph: bool = True) -> float:
+        ms = C.c_float()
+        self._c("qx_time_steps", nsteps, int(use_graph), C.byref(ms))
+        return ms.value
+
+    def profile_step(self, nsteps: int):
+        names = C.create_string_buffer(64 * 16)
+        ms = np.zeros(16)
+        n = C.c_int()
+        self._c("qx_profile_step", nsteps, 16, names, _ptr(ms), C.byref(n))
+        raw = names.raw
+        return [(raw[64 * i:64 * i + 64].split(b"\0")[0].decode(), float(ms[i])) for i in range(n.value)]
+
+    def set_tune(self, x_rows: int = 0, y_tx: int = 0, la_tx: int = 0):
+        self._c("qx_set_tune", x_rows, y_tx, la_tx)
+
+    def device_pointers(self):
+        p, v = _vp(), _vp()
+        self._c("qx_device_pointers", C.byref(p), C.byref(v))
+        return p.value, v.value
+
+    def sync(self):
+        self._c("qx_sync")

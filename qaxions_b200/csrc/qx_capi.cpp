@@ -1,0 +1,284 @@
+// qx_capi.cpp -- extern "C" boundary over qx::Field (include/qaxions_b200.h).
+// Exceptions are caught here and turned into status codes + messages.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <fstream>
+#include <new>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/qaxions_b200.h"
+#include "qx_field.hpp"
+
+struct qx_field_s {
+    std::unique_ptr<qx::Field> f;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+int guarded(qx_field_t* h, F&& fn) {
+    if (!h || !h->f) {
+        g_err = "null or destroyed qx_field handle";
+        return QX_ERR_INVALID;
+    }
+    try {
+        fn(*h->f);
+        h->err.clear();
+        return QX_OK;
+    } catch (const std::invalid_argument& e) {
+        h->err = e.what();
+        return QX_ERR_INVALID;
+    } catch (const std::bad_alloc&) {
+        h->err = "device allocation failed";
+        return QX_ERR_NOMEM;
+    } catch (const std::logic_error& e) {
+        h->err = e.what();
+        return QX_ERR_STATE;
+    } catch (const std::runtime_error& e) {
+        h->err = e.what();
+        return QX_ERR_CUDA;
+    } catch (...) {
+        h->err = "unknown error";
+        return QX_ERR_INTERNAL;
+    }
+}
+
+void need(bool ok, const char* msg) {
+    if (!ok) throw std::invalid_argument(msg);
+}
+}  // namespace
+
+extern "C" {
+
+int qx_version(void) { return 100; }
+
+const char* qx_last_error(const qx_field_t* h) {
+    if (h && !h->err.empty()) return h->err.c_str();
+    return g_err.c_str();
+}
+
+int qx_set_device(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+        return e == cudaErrorInvalidDevice ? QX_ERR_INVALID : QX_ERR_CUDA;
+    }
+    g_err.clear();
+    return QX_OK;
+}
+
+int qx_create(int dim, int N, double L, double pref, double rho_mean, int dtype, int k0_policy, double dt,
+              qx_field_t** out) {
+    if (!out) {
+        g_err = "out must not be NULL";
+        return QX_ERR_INVALID;
+    }
+    *out = nullptr;
+    if (dtype != QX_C128 && dtype != QX_C64) {
+        g_err = "dtype must be QX_C128 or QX_C64";
+        return QX_ERR_INVALID;
+    }
+    if (k0_policy != QX_K0_REFERENCE && k0_policy != QX_K0_ZERO) {
+        g_err = "k0_policy must be QX_K0_REFERENCE or QX_K0_ZERO";
+        return QX_ERR_INVALID;
+    }
+    qx::FieldConfig c;
+    c.dim = dim;
+    c.N = N;
+    c.L = L;
+    c.pref = pref;
+    c.rho_mean = rho_mean;
+    c.prec = dtype == QX_C128 ? qx::Prec::F64 : qx::Prec::F32;
+    c.k0 = k0_policy == QX_K0_REFERENCE ? qx::K0::Reference : qx::K0::Zero;
+    c.dt = dt;
+    try {
+        auto h = new qx_field_s();
+        try {
+            h->f = qx::make_field(c);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        g_err.clear();
+        return QX_OK;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return QX_ERR_INVALID;
+    } catch (const std::bad_alloc&) {
+        g_err = "device allocation failed";
+        return QX_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return QX_ERR_CUDA;
+    }
+}
+
+int qx_destroy(qx_field_t* h) {
+    if (!h) return QX_OK;
+    try {
+        h->f.reset();
+    } catch (...) {
+    }
+    delete h;
+    return QX_OK;
+}
+
+int qx_set_dt(qx_field_t* h, double dt) { return guarded(h, [&](qx::Field& f) { f.set_dt(dt); }); }
+
+int qx_set_psi(qx_field_t* h, const double* p) {
+    return guarded(h, [&](qx::Field& f) { need(p, "psi is NULL"); f.set_psi(p); });
+}
+int qx_get_psi(qx_field_t* h, double* p) {
+    return guarded(h, [&](qx::Field& f) { need(p, "psi is NULL"); f.get_psi(p); });
+}
+int qx_set_V(qx_field_t* h, const double* v) {
+    return guarded(h, [&](qx::Field& f) { need(v, "V is NULL"); f.set_V(v); });
+}
+int qx_get_V(qx_field_t* h, double* v) {
+    return guarded(h, [&](qx::Field& f) { need(v, "V is NULL"); f.get_V(v); });
+}
+int qx_get_Vhat(qx_field_t* h, double* v) {
+    return guarded(h, [&](qx::Field& f) { need(v, "Vhat is NULL"); f.get_Vhat(v); });
+}
+int qx_set_Vhat(qx_field_t* h, const double* v) {
+    return guarded(h, [&](qx::Field& f) { need(v, "Vhat is NULL"); f.set_Vhat(v); });
+}
+
+int qx_kick(qx_field_t* h, double dt) { return guarded(h, [&](qx::Field& f) { f.kick(dt); f.sync(); }); }
+int qx_drift(qx_field_t* h, double dt) { return guarded(h, [&](qx::Field& f) { f.drift(dt); f.sync(); }); }
+int qx_poisson(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.Poisson(); f.sync(); }); }
+int qx_update_potential(qx_field_t* h) {
+    return guarded(h, [&](qx::Field& f) { f.updatePotential(); f.sync(); });
+}
+int qx_compute_energy(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.computeEnergy(); f.sync(); }); }
+int qx_update_time(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.updateTime(); }); }
+int qx_half_kick(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.half_kick(); f.sync(); }); }
+int qx_full_kick(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.full_kick(); f.sync(); }); }
+int qx_drift_update(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.drift_update(); f.sync(); }); }
+int qx_propagate(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.propagate(); f.sync(); }); }
+int qx_step(qx_field_t* h, int n) {
+    return guarded(h, [&](qx::Field& f) {
+        need(n >= 0, "nsteps must be >= 0");
+        f.step(n);
+        f.sync();
+    });
+}
+
+int qx_scalars(qx_field_t* h, double* vmax, double* rhomax, double* time, double* a, int* curr) {
+    return guarded(h, [&](qx::Field& f) {
+        if (vmax) *vmax = f.Vmax();
+        if (rhomax) *rhomax = f.rhomax();
+        if (time) *time = f.time();
+        if (a) *a = f.a();
+        if (curr) *curr = f.curr();
+    });
+}
+int qx_rho_stats(qx_field_t* h, double* rhomax, double* vmax) {
+    return guarded(h, [&](qx::Field& f) { f.rho_stats(rhomax, vmax); });
+}
+int qx_mass_energy(qx_field_t* h, double* M, double* E, double* K, double* W) {
+    return guarded(h, [&](qx::Field& f) { f.mass_energy(M, E, K, W); });
+}
+int qx_spectrum(qx_field_t* h, int source, int mode, int nbins, double* k, double* P, long long* count) {
+    return guarded(h, [&](qx::Field& f) {
+        need(source == 0 || source == 1, "source must be 0 (|psi|^2) or 1 (V)");
+        f.spectrum(source, mode, nbins, k, P, count);
+    });
+}
+
+int qx_fft_c2c(qx_field_t* h, double* data, int sign) {
+    return guarded(h, [&](qx::Field& f) {
+        need(data, "data is NULL");
+        need(sign == -1 || sign == 1, "sign must be -1 or +1");
+        f.host_c2c(data, sign);
+    });
+}
+int qx_fft_r2c(qx_field_t* h, const double* in, double* out) {
+    return guarded(h, [&](qx::Field& f) { need(in && out, "NULL buffer"); f.host_r2c(in, out); });
+}
+int qx_fft_c2r(qx_field_t* h, const double* in, double* out) {
+    return guarded(h, [&](qx::Field& f) { need(in && out, "NULL buffer"); f.host_c2r(in, out); });
+}
+
+int qx_ic_gaussian_solitons(qx_field_t* h, int n, const double* rows5, double bkg) {
+    return guarded(h, [&](qx::Field& f) {
+        need(n >= 0 && (n == 0 || rows5), "bad soliton table");
+        f.ic_gaussian_solitons(n, rows5, bkg);
+    });
+}
+
+// src/ic/solitons.cxx:32-50: one soliton per parsable 'amp sigma x y z' line
+int qx_ic_solitons_file(qx_field_t* h, const char* path, double bkg) {
+    return guarded(h, [&](qx::Field& f) {
+        need(path, "path is NULL");
+        std::ifstream in(path);
+        if (!in.is_open()) throw std::invalid_argument(std::string("Error opening file ") + path);
+        std::vector<double> rows;
+        std::string line;
+        while (std::getline(in, line)) {
+            std::istringstream ss(line);
+            double a, s, x, y, z;
+            if (ss >> a >> s >> x >> y >> z) rows.insert(rows.end(), {a, s, x, y, z});
+        }
+        f.ic_gaussian_solitons((int)(rows.size() / 5), rows.data(), bkg);
+    });
+}
+
+int qx_ic_config(qx_field_t* h, int kind, unsigned long long seed, int n_solitons, double rc_lo, double rc_hi,
+                 double sigma, double kc_factor, double clip, double rho0) {
+    return guarded(h, [&](qx::Field& f) {
+        need(kind == QX_IC_SOLITONS || kind == QX_IC_GRF, "kind must be QX_IC_SOLITONS or QX_IC_GRF");
+        need(n_solitons >= 0 && n_solitons <= 100000, "n_solitons out of range");
+        need(kind == QX_IC_GRF || n_solitons > 0, "a soliton IC needs n_solitons > 0");
+        f.ic_config(kind, seed, n_solitons, rc_lo, rc_hi, sigma, kc_factor, clip, rho0);
+    });
+}
+
+int qx_time_steps(qx_field_t* h, int nsteps, int use_graph, float* ms) {
+    return guarded(h, [&](qx::Field& f) {
+        need(ms, "ms is NULL");
+        *ms = f.time_steps(nsteps, use_graph);
+    });
+}
+
+int qx_profile_step(qx_field_t* h, int nsteps, int max_entries, char* names, double* ms, int* n_out) {
+    return guarded(h, [&](qx::Field& f) {
+        need(nsteps > 0 && names && ms && n_out, "bad profile arguments");
+        std::vector<std::pair<std::string, double>> r;
+        f.profile_step(nsteps, r);
+        const int n = (int)r.size() < max_entries ? (int)r.size() : max_entries;
+        for (int i = 0; i < n; ++i) {
+            std::strncpy(names + 64 * i, r[i].first.c_str(), 63);
+            names[64 * i + 63] = 0;
+            ms[i] = r[i].second;
+        }
+        *n_out = n;
+    });
+}
+
+int qx_set_tune(qx_field_t* h, int x_rows, int y_tx, int la_tx) {
+    return guarded(h, [&](qx::Field& f) {
+        need(x_rows >= 0 && y_tx >= 0 && la_tx >= 0, "tune values must be >= 0");
+        f.tune().x_rows = x_rows;
+        f.tune().y_tx = y_tx;
+        f.tune().la_tx = la_tx;
+    });
+}
+
+int qx_device_pointers(qx_field_t* h, void** psi, void** V) {
+    return guarded(h, [&](qx::Field& f) {
+        if (psi) *psi = f.psi_device();
+        if (V) *V = f.V_device();
+    });
+}
+
+int qx_sync(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.sync(); }); }
+
+}  // extern "C"

@@ -1,0 +1,222 @@
+// qx_fft.cuh -- device-side pencil FFT for sm_100a.
+//
+// One pencil (a 1D transform of length L) is processed by T = L/E threads,
+// each holding E complex values in registers.  The transform is a mixed-radix
+// Stockham autosort FFT (radices 2, 3, 4, 8): every stage applies twiddles and
+// E/r radix-r butterflies in registers, and consecutive stages exchange data
+// through shared memory.  Stage s with radix r and span Ns reads inputs
+// x[j + m L/r] and writes outputs y[(j/Ns) Ns r + j%Ns + m Ns]
+// (j = t + b T, m = 0..r-1), so the result comes out in natural order.
+//
+// The first stage's inputs (positions t + b T + m L/r0) and the last stage's
+// outputs (positions t + b T + m L/r_last) are both lane-contiguous, so the
+// callers load the first stage straight from HBM and store the last stage
+// straight to HBM with coalesced accesses; only the S-1 inner exchanges touch
+// shared memory.
+//
+// Twiddles come from a table tw[i] = exp(-2 pi i i / L) evaluated in long
+// double on the host and rounded once to the storage precision.
+//
+// This replaces the FFTW c2c/r2c/c2r transforms of the reference's FFT plugin
+// (src/fft/fft.h:122-140): same unnormalised definitions, FORWARD = exp(-i..).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace qx {
+
+template <typename R> struct Cx;
+template <> struct Cx<float> { using T = float2; };
+template <> struct Cx<double> { using T = double2; };
+
+template <typename R> using cx_t = typename Cx<R>::T;
+
+template <typename C> __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) { C c; c.x = a; c.y = b; return c; }
+
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+    return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * s, a.y * s); }
+// multiply by sign*i: sign=-1 -> -i, sign=+1 -> +i
+template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
+    return SIGN < 0 ? mk<C>(a.y, -a.x) : mk<C>(-a.y, a.x);
+}
+
+// ---------------------------------------------------------------------------
+// Radix plans (compile time).  L = 2^e: [2^(e%3) if e%3] + [8]*(e/3) (e <= 3:
+// one stage of radix L).  L = 3*2^k: [4]*(k/2) + [2]*(k%2) + [3].
+// ---------------------------------------------------------------------------
+
+__host__ __device__ constexpr bool qx_is_pow2(int L) { return L > 0 && (L & (L - 1)) == 0; }
+__host__ __device__ constexpr int qx_log2(int L) { return L <= 1 ? 0 : 1 + qx_log2(L / 2); }
+
+__host__ __device__ constexpr int qx_nstages(int L) {
+    return qx_is_pow2(L) ? (qx_log2(L) <= 3 ? 1 : (qx_log2(L) / 3 + (qx_log2(L) % 3 ? 1 : 0)))
+                         : (qx_log2(L / 3) / 2 + qx_log2(L / 3) % 2 + 1);
+}
+
+__host__ __device__ constexpr int qx_radix(int L, int s) {
+    if (qx_is_pow2(L)) {
+        const int e = qx_log2(L);
+        if (e <= 3) return L;
+        const int rem = e % 3;
+        if (rem) return s == 0 ? (1 << rem) : 8;
+        return 8;
+    }
+    const int k = qx_log2(L / 3);
+    const int n4 = k / 2, n2 = k % 2;
+    if (s < n4) return 4;
+    if (s < n4 + n2) return 2;
+    return 3;
+}
+
+__host__ __device__ constexpr int qx_span(int L, int s) {  // product of radices before stage s
+    return s == 0 ? 1 : qx_span(L, s - 1) * qx_radix(L, s - 1);
+}
+
+__host__ __device__ constexpr int qx_gcd(int a, int b) { return b == 0 ? a : qx_gcd(b, a % b); }
+__host__ __device__ constexpr int qx_lcm(int a, int b) { return a / qx_gcd(a, b) * b; }
+__host__ __device__ constexpr int qx_lcm_radices(int L, int s = 0) {
+    return s >= qx_nstages(L) ? 1 : qx_lcm(qx_radix(L, s), qx_lcm_radices(L, s + 1));
+}
+
+// Elements per thread for a row pass that holds both an N-point c2c and the
+// N/2-point core of an r2c/c2r: E_half = lcm(radices(N/2)), E_full = 2 E_half.
+__host__ __device__ constexpr int qx_row_efull(int N) { return 2 * qx_lcm_radices(N / 2); }
+__host__ __device__ constexpr int qx_row_threads(int N) { return N / qx_row_efull(N); }
+
+// ---------------------------------------------------------------------------
+// Small DFT codelets (SIGN = -1 forward, +1 backward), in place on a[0..r-1].
+// ---------------------------------------------------------------------------
+
+template <typename R> struct Consts {
+    static constexpr R rsqrt2 = R(0.70710678118654752440084436210484903928);
+    static constexpr R sqrt3_2 = R(0.86602540378443864676372317075293618347);
+};
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft2(C* a) {
+    C t = a[0];
+    a[0] = cadd(t, a[1]);
+    a[1] = csub(t, a[1]);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft4(C* a) {
+    C t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
+    C t2 = cadd(a[1], a[3]), t3 = cmul_si<SIGN>(csub(a[1], a[3]));
+    a[0] = cadd(t0, t2);
+    a[2] = csub(t0, t2);
+    a[1] = cadd(t1, t3);
+    a[3] = csub(t1, t3);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* a) {
+    using R = decltype(C::x);
+    const C s = cadd(a[1], a[2]);
+    const C d = csub(a[1], a[2]);
+    const C m = mk<C>(a[0].x - R(0.5) * s.x, a[0].y - R(0.5) * s.y);
+    const C rot = cmul_si<SIGN>(cscale(d, Consts<R>::sqrt3_2));
+    a[0] = cadd(a[0], s);
+    a[1] = cadd(m, rot);
+    a[2] = csub(m, rot);
+}
+
+template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* a) {
+    using R = decltype(C::x);
+    C e[4] = {a[0], a[2], a[4], a[6]};
+    C o[4] = {a[1], a[3], a[5], a[7]};
+    dft4<SIGN>(e);
+    dft4<SIGN>(o);
+    const R h = Consts<R>::rsqrt2;
+    // o[q] *= W8^q (sign SIGN): W8^1 = h(1 + SIGN i), W8^2 = SIGN i, W8^3 = h(-1 + SIGN i)
+    const C o1 = o[1], o3 = o[3];
+    o[1] = cscale(cadd(o1, cmul_si<SIGN>(o1)), h);
+    o[2] = cmul_si<SIGN>(o[2]);
+    o[3] = cscale(csub(cmul_si<SIGN>(o3), o3), h);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        a[q] = cadd(e[q], o[q]);
+        a[q + 4] = csub(e[q], o[q]);
+    }
+}
+
+template <int r, int SIGN, typename C> __device__ __forceinline__ void dft(C* a) {
+    if constexpr (r == 2) dft2<SIGN>(a);
+    else if constexpr (r == 3) dft3<SIGN>(a);
+    else if constexpr (r == 4) dft4<SIGN>(a);
+    else if constexpr (r == 8) dft8<SIGN>(a);
+    else static_assert(r == 2 || r == 3 || r == 4 || r == 8, "unsupported radix");
+}
+
+// ---------------------------------------------------------------------------
+// Stage driver.
+// Acc: shared-memory accessor with `C& operator()(int pos)` for this pencil and
+// a `sync()` that is a barrier over every thread sharing the buffer.
+// ---------------------------------------------------------------------------
+
+// position held in v[e] before stage s (stage-s input order)
+template <int L, int E, int s> __device__ __forceinline__ int in_pos(int e, int t) {
+    constexpr int r = qx_radix(L, s);
+    constexpr int T = L / E;
+    return t + (e / r) * T + (e % r) * (L / r);
+}
+// position held in v[e] after the last stage (natural-order output)
+template <int L, int E> __device__ __forceinline__ int out_pos(int e, int t) {
+    constexpr int r = qx_radix(L, qx_nstages(L) - 1);
+    constexpr int T = L / E;
+    return t + (e / r) * T + (e % r) * (L / r);
+}
+
+template <int L, int E, int SIGN, int s, typename C, typename Acc>
+__device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const C* __restrict__ tw) {
+    constexpr int S = qx_nstages(L);
+    if constexpr (s < S) {
+        constexpr int r = qx_radix(L, s);
+        constexpr int Ns = qx_span(L, s);
+        constexpr int T = L / E;
+        static_assert(E % r == 0, "radix must divide elements per thread");
+        constexpr int nb = E / r;
+#pragma unroll
+        for (int b = 0; b < nb; ++b) {
+            const int j = t + b * T;
+            if constexpr (Ns > 1) {
+                const int k = j % Ns;
+                constexpr int stw = L / (Ns * r);
+#pragma unroll
+                for (int m = 1; m < r; ++m) {
+                    C w = __ldg(&tw[k * m * stw]);
+                    if (SIGN > 0) w.y = -w.y;
+                    v[b * r + m] = cmul(v[b * r + m], w);
+                }
+            }
+            dft<r, SIGN>(&v[b * r]);
+        }
+        if constexpr (s + 1 < S) {
+            constexpr int r2 = qx_radix(L, s + 1);
+            acc.sync();
+#pragma unroll
+            for (int b = 0; b < nb; ++b) {
+                const int j = t + b * T;
+                const int idxD = (j / Ns) * Ns * r + (j % Ns);
+#pragma unroll
+                for (int m = 0; m < r; ++m) acc(idxD + m * Ns) = v[b * r + m];
+            }
+            acc.sync();
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<L, E, s + 1>(e, t));
+            fft_stages<L, E, SIGN, s + 1>(v, acc, t, tw);
+        }
+    }
+}
+
+// Full transform: v in stage-0 input order on entry (see in_pos<L,E,0>),
+// natural-order outputs at out_pos<L,E> on exit.
+template <int L, int E, int SIGN, typename C, typename Acc>
+__device__ __forceinline__ void fft_pencil(C (&v)[E], Acc& acc, int t, const C* __restrict__ tw) {
+    fft_stages<L, E, SIGN, 0>(v, acc, t, tw);
+}
+
+}  // namespace qx

@@ -1,0 +1,864 @@
+// qx_field.cpp -- implementation of the host Field / FFT plugin mirror.
+#include "qx_field.hpp"
+
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "qx_misc.hpp"
+#include "qx_philox.h"
+
+namespace qx {
+
+#define QX_CUDA(call)                                                                               \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_));           \
+    } while (0)
+
+static const double kTwoPi = 6.283185307179586476925286766559005768;
+
+// ---------------------------------------------------------------------------
+// device buffer
+// ---------------------------------------------------------------------------
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void alloc(size_t n) {
+        if (n == bytes && p) return;
+        release();
+        cudaError_t e = cudaMalloc(&p, n ? n : 1);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw std::bad_alloc();
+        }
+        bytes = n;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// host helpers: twiddles, packing, spectrum tables
+// ---------------------------------------------------------------------------
+
+template <typename C> static std::vector<C> twiddles(int L) {
+    std::vector<C> t(L);
+    const long double tp = 6.283185307179586476925286766559005768L;
+    for (int j = 0; j < L; ++j) {
+        const long double a = -tp * (long double)j / (long double)L;
+        t[j].x = (decltype(t[j].x))cosl(a);
+        t[j].y = (decltype(t[j].y))sinl(a);
+    }
+    return t;
+}
+
+static inline long mirror_row(int dim, int N, long r) {
+    if (dim == 2) return (N - r) % N;
+    const long y = r % N, z = r / N;
+    return ((N - z) % N) * N + (N - y) % N;
+}
+
+void pack_half(int dim, int N, const double* h, double* p) {
+    const long rows = dim == 3 ? (long)N * N : N;
+    const int X = N / 2, XH = N / 2 + 1;
+    for (long r = 0; r < rows; ++r) {
+        const double* hr = h + 2 * r * XH;
+        double* pr = p + 2 * r * X;
+        for (int k = 1; k < X; ++k) {
+            pr[2 * k] = hr[2 * k];
+            pr[2 * k + 1] = hr[2 * k + 1];
+        }
+        // col0 = A + i B, A = H[0], B = H[N/2]
+        const double ax = hr[0], ay = hr[1], bx = hr[2 * X], by = hr[2 * X + 1];
+        pr[0] = ax - by;
+        pr[1] = ay + bx;
+    }
+}
+
+void unpack_half(int dim, int N, const double* p, double* h) {
+    const long rows = dim == 3 ? (long)N * N : N;
+    const int X = N / 2, XH = N / 2 + 1;
+    for (long r = 0; r < rows; ++r) {
+        const double* pr = p + 2 * r * X;
+        const double* pm = p + 2 * mirror_row(dim, N, r) * X;
+        double* hr = h + 2 * r * XH;
+        for (int k = 1; k < X; ++k) {
+            hr[2 * k] = pr[2 * k];
+            hr[2 * k + 1] = pr[2 * k + 1];
+        }
+        const double cx = pr[0], cy = pr[1], mx = pm[0], my = -pm[1];  // conj C(-k)
+        hr[0] = 0.5 * (cx + mx);
+        hr[1] = 0.5 * (cy + my);
+        // B = (C - conj C(-k)) / (2i)
+        const double dx = cx - mx, dy = cy - my;
+        hr[2 * X] = 0.5 * dy;
+        hr[2 * X + 1] = -0.5 * dx;
+    }
+}
+
+std::vector<int> spectrum_bin_table(int dim, int N, int mode, int nbins) {
+    const int nmax = N / 2;
+    const long Mmax = (long)dim * nmax * nmax;
+    std::vector<int> tab(Mmax + 1, -1);
+    for (long M = 0; M <= Mmax; ++M) {
+        const double r = std::sqrt((double)M);
+        long b = -1;
+        if (mode == 0) {
+            b = std::lrint(r);
+            if (b >= nmax + 1) b = -1;
+        } else if (mode == 1) {
+            if (M > 0 && r < nmax) b = (long)std::floor(nbins * r / nmax);
+            if (b >= nbins) b = -1;
+        } else {
+            if (M > 0 && r < nmax) b = (long)std::floor(nbins * std::log(r) / std::log((double)nmax) + 1e-9);
+            if (b >= nbins) b = -1;
+        }
+        tab[M] = (int)b;
+    }
+    return tab;
+}
+
+std::vector<double> spectrum_k_axis(int N, int mode, int nbins, double L) {
+    const double dk = kTwoPi / L;
+    const int nmax = N / 2;
+    std::vector<double> k;
+    if (mode == 0) {
+        for (int b = 0; b <= nmax; ++b) k.push_back(b * dk);
+    } else if (mode == 1) {
+        for (int b = 0; b < nbins; ++b) k.push_back((b + 0.5) * nmax / nbins * dk);
+    } else {
+        for (int b = 0; b < nbins; ++b) k.push_back(std::pow((double)nmax, (b + 0.5) / nbins) * dk);
+    }
+    return k;
+}
+
+// ---------------------------------------------------------------------------
+// FFT plugin
+// ---------------------------------------------------------------------------
+
+template <typename R>
+static typename Ops<R>::XP xp0(const Geometry& g, const typename Ops<R>::C* twN, const typename Ops<R>::C* twM) {
+    typename Ops<R>::XP a{};
+    a.twN = twN;
+    a.twM = twM;
+    a.rows = g.rows;
+    a.scale = 1.0;
+    a.pref = 1.0;
+    a.rho_mean = 0.0;
+    return a;
+}
+
+template <typename R>
+static typename Ops<R>::SP sp0(const Geometry& g, typename Ops<R>::C* a, const typename Ops<R>::C* tw, int X) {
+    typename Ops<R>::SP s{};
+    s.a = a;
+    s.tw = tw;
+    s.X = X;
+    s.dim = g.dim;
+    s.N = g.N;
+    s.scale = 1.0;
+    return s;
+}
+
+template <typename R> void B200FFTBackend<R>::forward_c2c(void* data) {
+    C* d = static_cast<C*>(data);
+    auto a = xp0<R>(g_, twN_, twM_);
+    a.in = d;
+    a.out = d;
+    Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, d, twN_, g_.N), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(g_, d, twN_, g_.N), OP_FWD, *tune_, st_);
+}
+
+template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C* out) {
+    auto a = xp0<R>(g_, twN_, twM_);
+    a.in = in;
+    a.out = out;
+    Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, out, twN_, g_.N), -1, *tune_, st_);
+}
+
+template <typename R> void B200FFTBackend<R>::backward_c2c(void* data) {
+    C* d = static_cast<C*>(data);
+    Ops<R>::la_pass(g_.N, sp0<R>(g_, d, twN_, g_.N), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, d, twN_, g_.N), +1, *tune_, st_);
+    auto a = xp0<R>(g_, twN_, twM_);
+    a.in = d;
+    a.out = d;
+    Ops<R>::x_inv(g_.N, a, false, *tune_, st_);
+}
+
+template <typename R> void B200FFTBackend<R>::forward_r2c(void* in_real, void* out_half) {
+    C* h = static_cast<C*>(out_half);
+    auto a = xp0<R>(g_, twN_, twM_);
+    a.Vin = static_cast<const R*>(in_real);
+    a.vh = h;
+    Ops<R>::x_r2c(g_.N, a, true, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, h, twN_, g_.N / 2), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(g_, h, twN_, g_.N / 2), OP_FWD, *tune_, st_);
+}
+
+template <typename R> void B200FFTBackend<R>::backward_c2r(void* in_half, void* out_real) {
+    C* h = static_cast<C*>(in_half);
+    Ops<R>::la_pass(g_.N, sp0<R>(g_, h, twN_, g_.N / 2), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, h, twN_, g_.N / 2), +1, *tune_, st_);
+    auto a = xp0<R>(g_, twN_, twM_);
+    a.vh = h;
+    a.Vout = static_cast<R*>(out_real);
+    Ops<R>::x_c2r(g_.N, a, C2R_WRITE_V, *tune_, st_);
+}
+
+template class B200FFTBackend<float>;
+template class B200FFTBackend<double>;
+
+// ---------------------------------------------------------------------------
+// Field
+// ---------------------------------------------------------------------------
+
+void Field::updateTime() {  // src/field.cxx:349-361 (STATIC cosmology: a = 1)
+    curr_ += 1;
+    s_ += ds_;
+}
+
+void Field::drift_update() {  // src/field.cxx:378-386
+    drift(ds_);
+    updateTime();
+    updatePotential();
+}
+
+void Field::propagate() {  // src/field.cxx:388-402
+    kick(0.5 * ds_);
+    drift(ds_);
+    updateTime();
+    updatePotential();
+    kick(0.5 * ds_);
+}
+
+template <typename R>
+class FieldT final : public Field {
+  public:
+    using C = typename Ops<R>::C;
+
+    explicit FieldT(const FieldConfig& cfg) {
+        cfg_ = cfg;
+        if (cfg.dim != 2 && cfg.dim != 3) throw std::invalid_argument("Dimension must be 2 or 3");
+        if (!supported_n(cfg.N)) throw std::invalid_argument("unsupported grid size N=" + std::to_string(cfg.N));
+        if (!(cfg.L > 0.0)) throw std::invalid_argument("box size L must be positive");
+        if (cfg.device >= 0) QX_CUDA(cudaSetDevice(cfg.device));
+        QX_CUDA(cudaGetDevice(&device_));
+        g_.dim = cfg.dim;
+        g_.N = cfg.N;
+        g_.rows = cfg.dim == 3 ? (long)cfg.N * cfg.N : cfg.N;
+        g_.S = g_.rows * cfg.N;
+        g_.hsites = g_.rows * (cfg.N / 2);
+        ds_ = cfg.dt;
+        QX_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+        psi_.alloc(sizeof(C) * g_.S);
+        V_.alloc(sizeof(R) * g_.S);
+        vh_.alloc(sizeof(C) * g_.hsites);
+        red_.alloc(sizeof(double) * 2 * kRedBlocks);
+        redout_.alloc(sizeof(double) * 4);
+        auto tN = twiddles<C>(cfg.N), tM = twiddles<C>(cfg.N / 2);
+        twN_.alloc(sizeof(C) * tN.size());
+        twM_.alloc(sizeof(C) * tM.size());
+        QX_CUDA(cudaMemcpy(twN_.p, tN.data(), sizeof(C) * tN.size(), cudaMemcpyHostToDevice));
+        QX_CUDA(cudaMemcpy(twM_.p, tM.data(), sizeof(C) * tM.size(), cudaMemcpyHostToDevice));
+        QX_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, st_));
+        QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
+        QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
+        fft_ = std::make_unique<B200FFTBackend<R>>(g_, twN_.as<C>(), twM_.as<C>(), &tune_, st_);
+        QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    ~FieldT() override {
+        drop_graph();
+        if (st_) {
+            cudaStreamSynchronize(st_);
+            cudaStreamDestroy(st_);
+        }
+    }
+
+    // ---- derived constants ----
+    double dk() const { return kTwoPi / cfg_.L; }
+    double pois_c() const { return -1.0 / (dk() * dk() * (double)g_.S); }
+    double pois_g0() const { return cfg_.k0 == K0::Reference ? -1.0 / (double)g_.S : 0.0; }
+    C* psi() { return psi_.as<C>(); }
+    R* V() { return V_.as<R>(); }
+    C* vh() { return vh_.as<C>(); }
+
+    typename Ops<R>::XP xp() { return xp0<R>(g_, twN_.as<C>(), twM_.as<C>()); }
+    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(g_, a, twN_.as<C>(), X); }
+
+    // ---- pass sequences ----
+    void y_fwd(C* a, int X) {
+        if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp(a, X), -1, tune_, st_);
+    }
+    void y_inv(C* a, int X) {
+        if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp(a, X), +1, tune_, st_);
+    }
+    void la_drift(double dt) {
+        auto s = sp(psi(), g_.N);
+        s.phase_fac = -0.5 * dt * dk() * dk();
+        s.scale = 1.0 / (double)g_.S;
+        Ops<R>::la_pass(g_.N, s, OP_DRIFT, tune_, st_);
+    }
+    void la_poisson() {
+        auto s = sp(vh(), g_.N / 2);
+        s.pois_c = pois_c();
+        s.pois_g0 = pois_g0();
+        Ops<R>::la_pass(g_.N, s, OP_POISSON, tune_, st_);
+    }
+    // density source -> half spectrum, transformed along all axes but the
+    // last (ready for the fused last-axis Poisson pass)
+    void density_r2c_partial() {
+        auto a = xp();
+        a.in = psi();
+        a.vh = vh();
+        a.pref = cfg_.pref;
+        a.rho_mean = cfg_.rho_mean;
+        Ops<R>::x_r2c(g_.N, a, false, tune_, st_);
+        y_fwd(vh(), g_.N / 2);
+    }
+
+    // ---- reference operator surface ----
+    void kick(double dt) override { Misc<R>::kick(psi(), V(), dt, g_.S, st_); }
+
+    void drift(double dt) override {  // src/field.cxx:119-198
+        auto a = xp();
+        a.in = psi();
+        a.out = psi();
+        Ops<R>::x_fwd(g_.N, a, false, tune_, st_);
+        y_fwd(psi(), g_.N);
+        la_drift(dt);
+        y_inv(psi(), g_.N);
+        Ops<R>::x_inv(g_.N, a, false, tune_, st_);
+        v_current_ = false;
+    }
+
+    void Poisson() override { Misc<R>::poisson_packed(vh(), g_.dim, g_.N, pois_c(), pois_g0(), st_); }
+
+    void updatePotential() override {  // src/field.cxx:294-346
+        density_r2c_partial();
+        la_poisson();
+        y_inv(vh(), g_.N / 2);
+        auto a = xp();
+        a.vh = vh();
+        a.Vout = V();
+        Ops<R>::x_c2r(g_.N, a, C2R_WRITE_V, tune_, st_);
+        v_current_ = true;
+        vmax_ = reduce(RED_VABS)[1];
+    }
+
+    void computeEnergy() override {  // src/field.cxx:200-227 (overwrites V with rho)
+        Misc<R>::rho_to_V(psi(), V(), g_.S, st_);
+        auto r = reduce(RED_RHO);
+        rhomax_ = r[1] / (r[0] / (double)g_.S);
+        v_current_ = false;
+    }
+
+    // fused merged leapfrog (src/main.cxx:64-85)
+    void step(int nsteps) override {
+        if (nsteps <= 0) return;
+        // prologue: potential of psi, half kick, forward x transform
+        density_r2c_partial();
+        la_poisson();
+        y_inv(vh(), g_.N / 2);
+        {
+            auto a = xp();
+            a.in = psi();
+            a.out = psi();
+            a.vh = vh();
+            a.Vout = V();
+            a.dt = 0.5 * ds_;
+            Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_);
+        }
+        // body: psi^_x -> drift -> psi, rho^ -> Poisson -> kick -> psi^_x
+        for (int i = 0; i < nsteps - 1; ++i) {
+            if (graph_enabled_) {
+                if (!graph_exec_ || graph_dt_ != ds_) capture_body();
+                QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
+            } else {
+                body(ds_, false);
+            }
+        }
+        body(ds_, true);
+        curr_ += nsteps;
+        s_ += nsteps * ds_;
+        v_current_ = true;
+        vmax_stale_ = true;
+    }
+
+    // one loop iteration; last = final half kick, psi in real space, V written
+    void body(double dt, bool last) {
+        y_fwd(psi(), g_.N);
+        la_drift(dt);
+        y_inv(psi(), g_.N);
+        auto a = xp();
+        a.in = psi();
+        a.out = psi();
+        a.vh = vh();
+        a.Vout = V();
+        a.pref = cfg_.pref;
+        a.rho_mean = cfg_.rho_mean;
+        Ops<R>::x_inv(g_.N, a, true, tune_, st_);
+        y_fwd(vh(), g_.N / 2);
+        la_poisson();
+        y_inv(vh(), g_.N / 2);
+        if (last) {
+            a.dt = 0.5 * dt;
+            Ops<R>::x_c2r(g_.N, a, C2R_WRITE_V | C2R_KICK | C2R_WRITE_PSI, tune_, st_);
+        } else {
+            a.dt = dt;
+            Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_);
+        }
+    }
+
+    void capture_body() {
+        drop_graph();
+        // one eager launch first so kernel attributes are set outside capture
+        QX_CUDA(cudaStreamSynchronize(st_));
+        cudaGraph_t g;
+        QX_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        try {
+            body(ds_, false);
+        } catch (...) {
+            cudaStreamEndCapture(st_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        QX_CUDA(cudaStreamEndCapture(st_, &g));
+        QX_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
+        cudaGraphDestroy(g);
+        graph_dt_ = ds_;
+    }
+
+    void drop_graph() {
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+
+    // ---- reductions ----
+    std::vector<double> reduce(int kind) {
+        Misc<R>::reduce(kind, psi(), V(), g_.S, red_.as<double>(), redout_.as<double>(), st_);
+        double h[2];
+        QX_CUDA(cudaMemcpyAsync(h, redout_.p, sizeof(h), cudaMemcpyDeviceToHost, st_));
+        QX_CUDA(cudaStreamSynchronize(st_));
+        return {h[0], h[1]};
+    }
+
+    void rho_stats(double* rhomax, double* vmax) override {
+        auto r = reduce(RED_RHO);
+        rhomax_ = r[1] / (r[0] / (double)g_.S);
+        if (vmax_stale_) {
+            vmax_ = reduce(RED_VABS)[1];
+            vmax_stale_ = false;
+        }
+        if (rhomax) *rhomax = rhomax_;
+        if (vmax) *vmax = vmax_;
+    }
+
+    void ensure_V() {
+        if (!v_current_) updatePotential();
+    }
+
+    void mass_energy(double* M, double* E, double* K, double* W) override {
+        const double dV = std::pow(cfg_.L / g_.N, g_.dim);
+        const double m = reduce(RED_RHO)[0] * dV;
+        ensure_V();
+        const double w = 0.5 * dV * reduce(RED_VRHO)[0];
+        // kinetic: 1/2 dV/S sum k^2 |psi^|^2 with the last axis fused into the reduction
+        mpsi_.alloc(sizeof(C) * g_.S);
+        fft_->forward_c2c_partial(psi(), mpsi_.as<C>());
+        auto s = sp(mpsi_.as<C>(), g_.N);
+        const long nblk = Ops<R>::la_blocks(g_.N, g_.N, g_.dim, OP_KIN, tune_);
+        kin_.alloc(sizeof(double) * (nblk + 1));
+        s.partial = kin_.as<double>();
+        Ops<R>::la_pass(g_.N, s, OP_KIN, tune_, st_);
+        Misc<R>::fold_sum(kin_.as<double>(), nblk, redout_.as<double>(), st_);
+        double ks = 0.0;
+        QX_CUDA(cudaMemcpyAsync(&ks, redout_.p, sizeof(double), cudaMemcpyDeviceToHost, st_));
+        QX_CUDA(cudaStreamSynchronize(st_));
+        const double kin = 0.5 * dV / (double)g_.S * dk() * dk() * ks;
+        if (M) *M = m;
+        if (K) *K = kin;
+        if (W) *W = w;
+        if (E) *E = kin + w;
+    }
+
+    void spectrum(int source, int mode, int nbins, double* k, double* P, long long* count) override {
+        if (mode < 0 || mode > 2) throw std::invalid_argument("spectrum mode must be 0, 1 or 2");
+        if (mode == 0) nbins = g_.N / 2 + 1;
+        if (nbins <= 0 || nbins > 4096) throw std::invalid_argument("nbins out of range");
+        const long key = ((long)mode << 20) | nbins;
+        auto it = bintab_.find(key);
+        if (it == bintab_.end()) {
+            auto tab = spectrum_bin_table(g_.dim, g_.N, mode, nbins);
+            auto buf = std::make_unique<DevBuf>();
+            buf->alloc(sizeof(int) * tab.size());
+            QX_CUDA(cudaMemcpy(buf->p, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice));
+            it = bintab_.emplace(key, std::move(buf)).first;
+        }
+        mvh_.alloc(sizeof(C) * g_.hsites);
+        auto a = xp();
+        a.vh = mvh_.as<C>();
+        if (source == 0) {
+            a.in = psi();
+            a.pref = 1.0;
+            a.rho_mean = 0.0;
+            Ops<R>::x_r2c(g_.N, a, false, tune_, st_);
+        } else {
+            a.Vin = V();
+            Ops<R>::x_r2c(g_.N, a, true, tune_, st_);
+        }
+        y_fwd(mvh_.as<C>(), g_.N / 2);
+        Ops<R>::la_pass(g_.N, sp(mvh_.as<C>(), g_.N / 2), OP_FWD, tune_, st_);
+        const int nblk_max = 296;
+        specP_.alloc(sizeof(double) * (size_t)nblk_max * nbins + sizeof(double) * nbins);
+        specC_.alloc(sizeof(long long) * (size_t)nblk_max * nbins + sizeof(long long) * nbins);
+        double* partP = specP_.as<double>();
+        long long* partC = specC_.as<long long>();
+        const int nblk = Misc<R>::spectrum_bin(mvh_.as<C>(), g_.dim, g_.N, it->second->as<int>(), nbins, partP,
+                                               partC, st_);
+        double* outP = partP + (size_t)nblk_max * nbins;
+        long long* outC = partC + (size_t)nblk_max * nbins;
+        Misc<R>::spectrum_fold(partP, partC, nblk, nbins, outP, outC, st_);
+        std::vector<double> hp(nbins);
+        std::vector<long long> hc(nbins);
+        QX_CUDA(cudaMemcpyAsync(hp.data(), outP, sizeof(double) * nbins, cudaMemcpyDeviceToHost, st_));
+        QX_CUDA(cudaMemcpyAsync(hc.data(), outC, sizeof(long long) * nbins, cudaMemcpyDeviceToHost, st_));
+        QX_CUDA(cudaStreamSynchronize(st_));
+        const double S2 = (double)g_.S * (double)g_.S;
+        auto kax = spectrum_k_axis(g_.N, mode, nbins, cfg_.L);
+        for (int b = 0; b < nbins; ++b) {
+            const double p = hp[b] / S2;
+            if (P) P[b] = hc[b] > 0 ? p / (double)hc[b] : p;
+            if (count) count[b] = hc[b];
+            if (k) k[b] = kax[b];
+        }
+    }
+
+    // ---- host buffers ----
+    void stage_alloc(size_t bytes) { stage_.alloc(bytes); }
+
+    void set_psi(const double* h) override {
+        if constexpr (sizeof(R) == 8) {
+            QX_CUDA(cudaMemcpyAsync(psi_.p, h, sizeof(C) * g_.S, cudaMemcpyHostToDevice, st_));
+        } else {
+            const long chunk = 1L << 22;
+            stage_alloc(sizeof(double2) * chunk);
+            for (long o = 0; o < g_.S; o += chunk) {
+                const long n = std::min(chunk, g_.S - o);
+                QX_CUDA(cudaMemcpyAsync(stage_.p, h + 2 * o, sizeof(double2) * n, cudaMemcpyHostToDevice, st_));
+                Misc<R>::from_f64(stage_.as<double2>(), psi() + o, n, st_);
+            }
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+        v_current_ = false;
+        vmax_stale_ = true;
+    }
+
+    void get_psi(double* h) override { download_c(psi(), g_.S, h); }
+
+    void download_c(const C* d, long n_el, double* h) {
+        if constexpr (sizeof(R) == 8) {
+            QX_CUDA(cudaMemcpyAsync(h, d, sizeof(C) * n_el, cudaMemcpyDeviceToHost, st_));
+        } else {
+            const long chunk = 1L << 22;
+            stage_alloc(sizeof(double2) * chunk);
+            for (long o = 0; o < n_el; o += chunk) {
+                const long n = std::min(chunk, n_el - o);
+                Misc<R>::to_f64(d + o, stage_.as<double2>(), n, st_);
+                QX_CUDA(cudaMemcpyAsync(h + 2 * o, stage_.p, sizeof(double2) * n, cudaMemcpyDeviceToHost, st_));
+            }
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    void upload_c(const double* h, C* d, long n_el) {
+        if constexpr (sizeof(R) == 8) {
+            QX_CUDA(cudaMemcpyAsync(d, h, sizeof(C) * n_el, cudaMemcpyHostToDevice, st_));
+        } else {
+            const long chunk = 1L << 22;
+            stage_alloc(sizeof(double2) * chunk);
+            for (long o = 0; o < n_el; o += chunk) {
+                const long n = std::min(chunk, n_el - o);
+                QX_CUDA(cudaMemcpyAsync(stage_.p, h + 2 * o, sizeof(double2) * n, cudaMemcpyHostToDevice, st_));
+                Misc<R>::from_f64(stage_.as<double2>(), d + o, n, st_);
+            }
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    void upload_r(const double* h, R* d, long n_el) {
+        if constexpr (sizeof(R) == 8) {
+            QX_CUDA(cudaMemcpyAsync(d, h, sizeof(R) * n_el, cudaMemcpyHostToDevice, st_));
+        } else {
+            const long chunk = 1L << 23;
+            stage_alloc(sizeof(double) * chunk);
+            for (long o = 0; o < n_el; o += chunk) {
+                const long n = std::min(chunk, n_el - o);
+                QX_CUDA(cudaMemcpyAsync(stage_.p, h + o, sizeof(double) * n, cudaMemcpyHostToDevice, st_));
+                Misc<R>::real_from_f64(stage_.as<double>(), d + o, n, st_);
+            }
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    void download_r(const R* d, long n_el, double* h) {
+        if constexpr (sizeof(R) == 8) {
+            QX_CUDA(cudaMemcpyAsync(h, d, sizeof(R) * n_el, cudaMemcpyDeviceToHost, st_));
+        } else {
+            const long chunk = 1L << 23;
+            stage_alloc(sizeof(double) * chunk);
+            for (long o = 0; o < n_el; o += chunk) {
+                const long n = std::min(chunk, n_el - o);
+                Misc<R>::real_to_f64(d + o, stage_.as<double>(), n, st_);
+                QX_CUDA(cudaMemcpyAsync(h + o, stage_.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st_));
+            }
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    void set_V(const double* h) override {
+        upload_r(h, V(), g_.S);
+        vmax_stale_ = true;
+    }
+    void get_V(double* h) override { download_r(V(), g_.S, h); }
+
+    void get_Vhat(double* h) override {
+        std::vector<double> packed(2 * g_.hsites);
+        download_c(vh(), g_.hsites, packed.data());
+        unpack_half(g_.dim, g_.N, packed.data(), h);
+    }
+    void set_Vhat(const double* h) override {
+        std::vector<double> packed(2 * g_.hsites);
+        pack_half(g_.dim, g_.N, h, packed.data());
+        upload_c(packed.data(), vh(), g_.hsites);
+    }
+
+    // ---- FFT plugin on host buffers (uses the measurement scratch) ----
+    void host_c2c(double* data, int sign) override {
+        mpsi_.alloc(sizeof(C) * g_.S);
+        upload_c(data, mpsi_.as<C>(), g_.S);
+        if (sign < 0) fft_->forward_c2c(mpsi_.p);
+        else fft_->backward_c2c(mpsi_.p);
+        download_c(mpsi_.as<C>(), g_.S, data);
+    }
+    void host_r2c(const double* in, double* out) override {
+        mpsi_.alloc(sizeof(C) * g_.S);  // real staging inside the complex scratch
+        mvh_.alloc(sizeof(C) * g_.hsites);
+        upload_r(in, reinterpret_cast<R*>(mpsi_.p), g_.S);
+        fft_->forward_r2c(mpsi_.p, mvh_.p);
+        std::vector<double> packed(2 * g_.hsites);
+        download_c(mvh_.as<C>(), g_.hsites, packed.data());
+        unpack_half(g_.dim, g_.N, packed.data(), out);
+    }
+    void host_c2r(const double* in, double* out) override {
+        mpsi_.alloc(sizeof(C) * g_.S);
+        mvh_.alloc(sizeof(C) * g_.hsites);
+        std::vector<double> packed(2 * g_.hsites);
+        pack_half(g_.dim, g_.N, in, packed.data());
+        upload_c(packed.data(), mvh_.as<C>(), g_.hsites);
+        fft_->backward_c2r(mvh_.p, mpsi_.p);
+        download_r(reinterpret_cast<R*>(mpsi_.p), g_.S, out);
+    }
+    FFTBackend* fftBackend() override { return fft_.get(); }
+
+    // ---- initial conditions ----
+    void ic_gaussian_solitons(int n, const double* rows5, double bkg) override {
+        if constexpr (sizeof(R) == 8) {
+            DevBuf rows;
+            rows.alloc(sizeof(double) * 5 * (n > 0 ? n : 1));
+            if (n > 0) QX_CUDA(cudaMemcpy(rows.p, rows5, sizeof(double) * 5 * n, cudaMemcpyHostToDevice));
+            IC::gauss_rho(reinterpret_cast<double2*>(psi()), g_.dim, g_.N, cfg_.L, bkg, n, rows.as<double>(), st_);
+            const double mean = reduce(RED_RE)[0] / (double)g_.S;
+            IC::sqrt_div(reinterpret_cast<double2*>(psi()), g_.S, mean, st_);
+            QX_CUDA(cudaStreamSynchronize(st_));
+            v_current_ = false;
+            vmax_stale_ = true;
+        } else {
+            FieldConfig c = cfg_;
+            c.prec = Prec::F64;
+            FieldT<double> tmp(c);
+            tmp.ic_gaussian_solitons(n, rows5, bkg);
+            adopt_f64(tmp);
+        }
+    }
+
+    void ic_config(int kind, uint64_t seed, int n_sol, double rc_lo, double rc_hi, double sigma,
+                   double kc_factor, double clip, double rho0) override {
+        if constexpr (sizeof(R) == 8) {
+            double2* p = reinterpret_cast<double2*>(psi());
+            if (kind == 0) {
+                QX_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, st_));
+            } else {
+                IC::noise(p, g_.S, seed, st_);
+                fft_->forward_c2c(psi_.p);
+                IC::grf_filter(p, g_.dim, g_.N, dk(), kc_factor * g_.N * dk(), st_);
+                fft_->backward_c2c(psi_.p);
+                auto r = reduce(RED_RE2);
+                const double sd = std::sqrt(r[0] / (double)g_.S);
+                IC::grf_finish(p, g_.S, sigma / sd, clip, st_);
+            }
+            if (n_sol > 0) {
+                std::vector<double> par(7 * n_sol);
+                for (int j = 0; j < n_sol; ++j) {
+                    const U4 a = philox4x32_10((uint32_t)j, 0u, 1u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+                    const U4 b = philox4x32_10((uint32_t)j, 1u, 1u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+                    const double rc = rc_lo + (rc_hi - rc_lo) * u01(a.v[0]);
+                    const double ph = kTwoPi * u01(a.v[1]);
+                    par[7 * j] = rc * rc;
+                    par[7 * j + 1] = std::sqrt(rho0 / (rc * rc * rc * rc));
+                    par[7 * j + 2] = std::cos(ph);
+                    par[7 * j + 3] = std::sin(ph);
+                    par[7 * j + 4] = u01(b.v[0]);
+                    par[7 * j + 5] = u01(b.v[1]);
+                    par[7 * j + 6] = g_.dim == 3 ? u01(b.v[2]) : 0.0;
+                }
+                DevBuf dpar;
+                dpar.alloc(sizeof(double) * par.size());
+                QX_CUDA(cudaMemcpy(dpar.p, par.data(), sizeof(double) * par.size(), cudaMemcpyHostToDevice));
+                IC::add_schive(p, g_.dim, g_.N, cfg_.L, n_sol, dpar.as<double>(), st_);
+                QX_CUDA(cudaStreamSynchronize(st_));
+            }
+            auto r = reduce(RED_RHO);
+            Misc<double>::scale(psi(), 1.0 / std::sqrt(r[0] / (double)g_.S), g_.S, st_);
+            QX_CUDA(cudaStreamSynchronize(st_));
+            v_current_ = false;
+            vmax_stale_ = true;
+        } else {
+            FieldConfig c = cfg_;
+            c.prec = Prec::F64;
+            FieldT<double> tmp(c);
+            tmp.ic_config(kind, seed, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0);
+            adopt_f64(tmp);
+        }
+    }
+
+    void adopt_f64(FieldT<double>& src) {
+        QX_CUDA(cudaStreamSynchronize(src.stream()));
+        Misc<R>::from_f64(reinterpret_cast<const double2*>(src.psi_device()), psi(), g_.S, st_);
+        QX_CUDA(cudaStreamSynchronize(st_));
+        v_current_ = false;
+        vmax_stale_ = true;
+    }
+
+    // ---- timing ----
+    float time_steps(int nsteps, int use_graph) override {
+        graph_enabled_ = use_graph != 0;
+        if (graph_enabled_ && nsteps > 1 && (!graph_exec_ || graph_dt_ != ds_)) capture_body();
+        cudaEvent_t e0, e1;
+        QX_CUDA(cudaEventCreate(&e0));
+        QX_CUDA(cudaEventCreate(&e1));
+        QX_CUDA(cudaEventRecord(e0, st_));
+        step(nsteps);
+        QX_CUDA(cudaEventRecord(e1, st_));
+        QX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        QX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        graph_enabled_ = true;
+        return ms;
+    }
+
+    // per-pass device time of the loop body, averaged over nsteps bodies
+    void profile_step(int nsteps, std::vector<std::pair<std::string, double>>& out) override {
+        const bool d3 = g_.dim == 3;
+        std::vector<std::string> names;
+        if (d3) names.push_back("y_fwd(psi)");
+        names.push_back(d3 ? "z_drift(psi)" : "y_drift(psi)");
+        if (d3) names.push_back("y_inv(psi)");
+        names.push_back("x_inv_r2c(psi->rho^)");
+        if (d3) names.push_back("y_fwd(rho^)");
+        names.push_back(d3 ? "z_poisson(rho^)" : "y_poisson(rho^)");
+        if (d3) names.push_back("y_inv(rho^)");
+        names.push_back("x_c2r_kick_fwd");
+        const size_t np = names.size();
+        std::vector<cudaEvent_t> ev(np + 1);
+        for (auto& e : ev) QX_CUDA(cudaEventCreate(&e));
+        std::vector<double> acc(np, 0.0);
+        {  // the loop body expects the x-transformed state
+            auto a = xp();
+            a.in = psi();
+            a.out = psi();
+            Ops<R>::x_fwd(g_.N, a, false, tune_, st_);
+        }
+        for (int it = 0; it < nsteps; ++it) {
+            size_t k = 0;
+            QX_CUDA(cudaEventRecord(ev[0], st_));
+            auto mark = [&]() { QX_CUDA(cudaEventRecord(ev[++k], st_)); };
+            if (d3) { y_fwd(psi(), g_.N); mark(); }
+            la_drift(ds_); mark();
+            if (d3) { y_inv(psi(), g_.N); mark(); }
+            auto a = xp();
+            a.in = psi(); a.out = psi(); a.vh = vh(); a.Vout = V();
+            a.pref = cfg_.pref; a.rho_mean = cfg_.rho_mean; a.dt = ds_;
+            Ops<R>::x_inv(g_.N, a, true, tune_, st_); mark();
+            if (d3) { y_fwd(vh(), g_.N / 2); mark(); }
+            la_poisson(); mark();
+            if (d3) { y_inv(vh(), g_.N / 2); mark(); }
+            Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_); mark();
+            QX_CUDA(cudaEventSynchronize(ev[np]));
+            for (size_t j = 0; j < np; ++j) {
+                float ms = 0.f;
+                QX_CUDA(cudaEventElapsedTime(&ms, ev[j], ev[j + 1]));
+                acc[j] += ms;
+            }
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        out.clear();
+        for (size_t j = 0; j < np; ++j) out.emplace_back(names[j], acc[j] / nsteps);
+        // back to real space (the profiled steps advanced the state by nsteps
+        // full kicks and drifts)
+        restore_after_profile();
+    }
+
+    void restore_after_profile() {
+        // psi holds the x-transformed state after a full kick; undo the x
+        // transform (1/N) so the field is back in real space.
+        auto a = xp();
+        a.in = psi();
+        a.out = psi();
+        a.scale = 1.0 / (double)g_.N;
+        Ops<R>::x_inv(g_.N, a, false, tune_, st_);
+        QX_CUDA(cudaStreamSynchronize(st_));
+        v_current_ = false;
+        vmax_stale_ = true;
+    }
+
+    void* psi_device() override { return psi_.p; }
+    void* V_device() override { return V_.p; }
+    void sync() override { QX_CUDA(cudaStreamSynchronize(st_)); }
+
+  private:
+    int device_ = 0;
+    DevBuf psi_, V_, vh_, twN_, twM_, red_, redout_;
+    DevBuf mpsi_, mvh_, kin_, specP_, specC_, stage_;
+    std::map<long, std::unique_ptr<DevBuf>> bintab_;
+    std::unique_ptr<B200FFTBackend<R>> fft_;
+    bool v_current_ = false;
+    bool vmax_stale_ = true;
+    bool graph_enabled_ = true;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    double graph_dt_ = 0.0;
+};
+
+std::unique_ptr<Field> make_field(const FieldConfig& cfg) {
+    if (cfg.prec == Prec::F64) return std::make_unique<FieldT<double>>(cfg);
+    return std::make_unique<FieldT<float>>(cfg);
+}
+
+}  // namespace qx

@@ -1,0 +1,182 @@
+// qx_field.hpp -- C++ host mirror of the reference's Field / FFTBackend
+// operator surface, driving the sm_100a kernels on one CUDA stream.
+//
+//   reference                                  here
+//   FFTBackend (src/fft/fft.h:9-26)            qx::FFTBackend (device buffers)
+//   FFTWOpenMPBackend (src/fft/fft.h:28-149)   qx::B200FFTBackend<R>
+//   Field (src/field.h:13-97)                  qx::Field (abstract) / qx::FieldT<R>
+//
+// R = double is the plain FP64 (complex128) form; R = float is the fused FP32
+// (complex64) form, whose phase arguments, reductions and spectrum sums stay
+// FP64.  Device buffers are owned by the field; host data moves only through
+// set_*/get_* copies.  A field is bound to one stream and is not thread-safe.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "qx_ops.hpp"
+
+namespace qx {
+
+enum class Prec { F64 = 0, F32 = 1 };
+enum class K0 { Reference = 0, Zero = 1 };
+
+struct FieldConfig {
+    int dim = 3;
+    int N = 64;
+    double L = 1.0;
+    double pref = 1.0;      // Poisson source prefactor (reference: norm_ * a_, src/field.cxx:298)
+    double rho_mean = 1.0;  // background density (src/field.cxx:77)
+    Prec prec = Prec::F64;
+    K0 k0 = K0::Reference;
+    double dt = 1e-4;       // ds_ used by half_kick/full_kick/drift_update/step
+    int device = -1;        // CUDA device (-1: current)
+};
+
+// Device-side FFT plugin: in-place c2c, r2c into the packed half spectrum,
+// c2r from it (input overwritten), all unnormalised with FFTW's sign
+// conventions.  ksites() is the packed size N^(d-1) N/2: column 0 carries the
+// kx = 0 and kx = N/2 planes as A + iB.
+class FFTBackend {
+  public:
+    virtual ~FFTBackend() = default;
+    virtual void forward_c2c(void* data) = 0;
+    virtual void backward_c2c(void* data) = 0;
+    virtual void forward_r2c(void* in_real, void* out_half) = 0;
+    virtual void backward_c2r(void* in_half, void* out_real) = 0;
+    virtual size_t sites() const = 0;
+    virtual size_t ksites() const = 0;
+    virtual bool owns_zero_mode() const { return true; }
+    virtual bool owns_zero_mode_k() const { return true; }
+    virtual ptrdiff_t global_N() const = 0;
+};
+
+struct Geometry {
+    int dim, N;
+    long S, rows, hsites;
+    long fftw_ksites() const { return rows * (N / 2 + 1); }
+};
+
+template <typename R>
+class B200FFTBackend : public FFTBackend {
+  public:
+    using C = typename Ops<R>::C;
+    B200FFTBackend(const Geometry& g, const C* twN, const C* twM, const Tune* tune, cudaStream_t st)
+        : g_(g), twN_(twN), twM_(twM), tune_(tune), st_(st) {}
+    void forward_c2c(void* data) override;
+    void backward_c2c(void* data) override;
+    void forward_r2c(void* in_real, void* out_half) override;
+    void backward_c2r(void* in_half, void* out_real) override;
+    size_t sites() const override { return (size_t)g_.S; }
+    size_t ksites() const override { return (size_t)g_.hsites; }
+    ptrdiff_t global_N() const override { return g_.N; }
+    // out-of-place forward c2c along all axes except the last, used by the
+    // kinetic-energy measurement (last axis fused with the reduction)
+    void forward_c2c_partial(const C* in, C* out);
+
+  private:
+    Geometry g_;
+    const C* twN_;
+    const C* twM_;
+    const Tune* tune_;
+    cudaStream_t st_;
+};
+
+class Field {
+  public:
+    virtual ~Field() = default;
+
+    // ---- reference operator surface (src/field.h:24-34) ----
+    virtual void kick(double dt) = 0;
+    virtual void drift(double dt) = 0;
+    virtual void Poisson() = 0;           // on the transformed packed V^ (after forward_r2c)
+    virtual void updatePotential() = 0;
+    virtual void computeEnergy() = 0;     // reference semantics: V <- |psi|^2, rhomax
+    void updateTime();
+    void half_kick() { kick(0.5 * ds_); }
+    void full_kick() { kick(ds_); }
+    void drift_update();
+    void propagate();
+    // merged leapfrog of src/main.cxx:64-85 (measurements off), fused passes,
+    // loop body replayed from a CUDA graph
+    virtual void step(int nsteps) = 0;
+
+    // ---- buffers (host FP64, reference index order) ----
+    virtual void set_psi(const double* interleaved) = 0;
+    virtual void get_psi(double* interleaved) = 0;
+    virtual void set_V(const double* v) = 0;
+    virtual void get_V(double* v) = 0;
+    virtual void get_Vhat(double* fftw_half) = 0;   // unpacked to FFTW's N/2+1 layout
+    virtual void set_Vhat(const double* fftw_half) = 0;
+
+    // ---- FFT plugin on host buffers ----
+    virtual void host_c2c(double* data, int sign) = 0;
+    virtual void host_r2c(const double* in, double* out_fftw_half) = 0;
+    virtual void host_c2r(const double* in_fftw_half, double* out) = 0;
+    virtual FFTBackend* fftBackend() = 0;
+
+    // ---- measurements (non-destructive) ----
+    virtual void rho_stats(double* rhomax, double* vmax) = 0;
+    virtual void mass_energy(double* M, double* E, double* K, double* W) = 0;
+    // shell-binned spectrum; source 0 = |psi|^2, 1 = V
+    virtual void spectrum(int source, int mode, int nbins, double* k, double* P, long long* count) = 0;
+
+    // ---- initial conditions (generated in FP64 on the device) ----
+    virtual void ic_gaussian_solitons(int n, const double* rows5, double bkg) = 0;
+    virtual void ic_config(int kind, uint64_t seed, int n_sol, double rc_lo, double rc_hi, double sigma,
+                           double kc_factor, double clip, double rho0) = 0;
+
+    // ---- timing / device access ----
+    virtual float time_steps(int nsteps, int use_graph) = 0;  // device ms of step(nsteps)
+    virtual void profile_step(int nsteps, std::vector<std::pair<std::string, double>>& per_kernel_ms) = 0;
+    virtual void* psi_device() = 0;
+    virtual void* V_device() = 0;
+    virtual void sync() = 0;
+    cudaStream_t stream() const { return st_; }
+
+    // ---- scalars ----
+    const FieldConfig& config() const { return cfg_; }
+    const Geometry& geom() const { return g_; }
+    int size() const { return cfg_.N; }
+    int dim() const { return cfg_.dim; }
+    double Lbox() const { return cfg_.L; }
+    size_t sites() const { return (size_t)g_.S; }
+    size_t ksites() const { return (size_t)g_.fftw_ksites(); }
+    double Vmax() { return vmax_; }
+    double rhomax() const { return rhomax_; }
+    double rho_mean() const { return cfg_.rho_mean; }
+    int curr() const { return curr_; }
+    double time() const { return s_; }
+    double a() const { return a_; }
+    double dt() const { return ds_; }
+    void set_dt(double dt) { ds_ = dt; }
+    Tune& tune() { return tune_; }
+
+  protected:
+    FieldConfig cfg_;
+    Geometry g_{};
+    cudaStream_t st_ = nullptr;
+    Tune tune_;
+    int curr_ = 0;
+    double s_ = 0.0, a_ = 1.0, ds_ = 0.0;
+    double vmax_ = 0.0, rhomax_ = 0.0;
+};
+
+std::unique_ptr<Field> make_field(const FieldConfig& cfg);
+
+// host-side conversion between FFTW's r2c layout and the packed layout
+void pack_half(int dim, int N, const double* fftw_half, double* packed);
+void unpack_half(int dim, int N, const double* packed, double* fftw_half);
+
+// spectrum bin of every integer |n|^2 (mode 0 reference shells, 1 linear, 2 log)
+std::vector<int> spectrum_bin_table(int dim, int N, int mode, int nbins);
+std::vector<double> spectrum_k_axis(int N, int mode, int nbins, double L);
+
+}  // namespace qx

@@ -1,0 +1,525 @@
+// qx_kernels.cuh -- pass kernels of the Schroedinger-Poisson step on sm_100a.
+//
+// Data layout in HBM (reference order, x fastest; src/ic/solitons.cxx:69-71):
+//   psi  [N^d]       complex (float2 for the fused FP32 form, double2 for FP64)
+//   vh   [N^(d-1) N/2] complex: r2c half spectrum with the self-conjugate
+//        kx = N/2 plane packed into column 0 (col0 = X[kx=0] + i X[kx=N/2]
+//        after the x transform; linear through the y/z transforms)
+//   V    [N^d]       real potential
+// A 3D transform is three passes over HBM: an x pass over contiguous rows, a
+// y pass over tiles of TX columns x N rows, and a last-axis (z) pass over tiles
+// of TX columns x N planes.  In 2D the y pass is the last axis.  Pointwise
+// work is fused into the passes:
+//   x passes    kick exp(-i dt V) before the forward x FFT; |psi|^2 density
+//               and the real-to-complex x FFT after the inverse x FFT; the
+//               complex-to-real x FFT, the kick and the next forward x FFT
+//   last axis   drift phase exp(-i dt k^2/2)/S between the forward and inverse
+//               transforms; Poisson divide -1/(k^2 S) between them on vh
+// Reference operations replaced: Field::kick/drift/Poisson/updatePotential
+// (src/field.cxx:93-346) and the FFTW plugin transforms (src/fft/fft.h:122-140).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "qx_fft.cuh"
+
+namespace qx {
+
+// ---------------------------------------------------------------------------
+// shared-memory accessors
+// ---------------------------------------------------------------------------
+
+// contiguous row, one padding element per 8 (bank-conflict-free stride-8 and
+// stride-64 exchanges for 8- and 16-byte elements)
+template <typename C> struct RowAcc {
+    C* base;
+    __device__ __forceinline__ C& operator()(int p) const { return base[p + (p >> 3)]; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+__host__ __device__ constexpr int row_smem_elems(int n) { return n + (n >> 3) + 1; }
+
+// column of a strided tile: element p of this pencil at base[p * pitch]
+template <typename C> struct ColAcc {
+    C* base;
+    int pitch;
+    __device__ __forceinline__ C& operator()(int p) const { return base[p * pitch]; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// ---------------------------------------------------------------------------
+// phase helpers: arguments in FP64, reduced mod 2 pi, then sin/cos in R
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ double reduce_2pi(double phi) {
+    const double inv2pi = 0.15915494309189533576888376337251436;
+    const double twopi = 6.283185307179586476925286766559005768;
+    return fma(-twopi, rint(phi * inv2pi), phi);
+}
+
+template <typename R> __device__ __forceinline__ cx_t<R> cis(double phi);
+template <> __device__ __forceinline__ float2 cis<float>(double phi) {
+    float s, c;
+    sincosf((float)reduce_2pi(phi), &s, &c);
+    return make_float2(c, s);
+}
+template <> __device__ __forceinline__ double2 cis<double>(double phi) {
+    double s, c;
+    sincos(reduce_2pi(phi), &s, &c);
+    return make_double2(c, s);
+}
+
+// psi * exp(-i dt V)   (src/field.cxx:100-112)
+template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, double dt) {
+    return cmul(p, cis<R>(-dt * (double)v));
+}
+
+__device__ __forceinline__ int signed_mode(int i, int N) { return i <= (N >> 1) ? i : i - N; }
+
+// ---------------------------------------------------------------------------
+// deterministic block reductions (fixed tree, FP64)
+// ---------------------------------------------------------------------------
+
+template <int OP>  // 0 sum, 1 max
+__device__ __forceinline__ double red_op(double a, double b) { return OP == 0 ? a + b : fmax(a, b); }
+
+template <int OP>
+__device__ double block_reduce(double v, double* red) {
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    if ((nthr & 31) == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = red_op<OP>(v, __shfl_xor_sync(0xffffffffu, v, o));
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = v;
+        __syncthreads();
+        double r = red[0];
+        for (int w = 1; w < (nthr >> 5); ++w) r = red_op<OP>(r, red[w]);
+        __syncthreads();
+        return r;
+    }
+    __syncthreads();
+    red[tid] = v;
+    __syncthreads();
+    double r = red[0];
+    for (int w = 1; w < nthr; ++w) r = red_op<OP>(r, red[w]);
+    __syncthreads();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// x passes (contiguous rows).  blockDim = (T, P): T = qx_row_threads(N)
+// threads per row, P rows per block.  Dynamic smem: P * row_smem_elems(N) C.
+// ---------------------------------------------------------------------------
+
+template <typename R> struct XArgs {
+    const cx_t<R>* in;      // complex rows of N (psi or psi^_x)
+    cx_t<R>* out;           // complex rows of N
+    cx_t<R>* vh;            // packed half rows of N/2
+    const R* Vin;           // real rows of N (potential for the kick / r2c source)
+    R* Vout;                // real rows of N
+    const cx_t<R>* twN;     // exp(-2 pi i j/N), j < N
+    const cx_t<R>* twM;     // exp(-2 pi i j/(N/2)), j < N/2
+    long rows;
+    double dt;              // kick time step
+    double pref, rho_mean;  // r2c source pref*(|psi|^2 - rho_mean)
+    double scale;           // applied after an inverse c2c (1/S when requested)
+};
+
+enum XFwdMode { XF_PLAIN = 0, XF_KICK = 1 };
+
+// forward c2c along x; optional kick by V first.  (Field::kick + first FFT pass)
+template <int N, typename R, int MODE>
+__global__ void k_x_fwd(XArgs<R> a) {
+    using C = cx_t<R>;
+    constexpr int E = qx_row_efull(N);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    const int t = threadIdx.x;
+    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
+    const C* src = a.in + row * N;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int p = in_pos<N, E, 0>(e, t);
+        v[e] = src[p];
+        if constexpr (MODE == XF_KICK) v[e] = kick1<R>(v[e], a.Vin[row * N + p], a.dt);
+    }
+    RowAcc<C> acc{sm};
+    fft_pencil<N, E, -1>(v, acc, t, a.twN);
+    C* dst = a.out + row * N;
+#pragma unroll
+    for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
+}
+
+// r2c post-processing of one row held in smem (Z[k], k < M) -> packed X row.
+// X[k] = (A + B)/2 - i W_N^k (A - B)/2, A = Z[k], B = conj(Z[M-k]);
+// col 0 = (Re Z0 + Im Z0) + i (Re Z0 - Im Z0) = X[0] + i X[N/2].
+template <int N, typename R>
+__device__ __forceinline__ void r2c_post_store(RowAcc<cx_t<R>>& acc, int t, cx_t<R>* dst, const cx_t<R>* twN) {
+    using C = cx_t<R>;
+    constexpr int M = N / 2;
+    constexpr int T = qx_row_threads(N);
+#pragma unroll
+    for (int i = 0; i < M / T; ++i) {
+        const int k = t + i * T;
+        const C A = acc(k);
+        C x;
+        if (k == 0) {
+            x = mk<C>(A.x + A.y, A.x - A.y);
+        } else {
+            const C B = cconj(acc(M - k));
+            const C s = cadd(A, B), d = csub(A, B);
+            const C w = __ldg(&twN[k]);
+            // -i * w * d
+            const C wd = cmul(w, d);
+            x = mk<C>(R(0.5) * (s.x + wd.y), R(0.5) * (s.y - wd.x));
+        }
+        dst[k] = x;
+    }
+}
+
+enum XInvMode { XI_PLAIN = 0, XI_R2C = 1 };
+
+// inverse c2c along x (psi^_x -> psi, times scale); optionally the density
+// source pref(|psi|^2 - rho_mean) and its r2c x transform into vh.
+template <int N, typename R, int MODE>
+__global__ void k_x_inv(XArgs<R> a) {
+    using C = cx_t<R>;
+    constexpr int E = qx_row_efull(N);
+    constexpr int M = N / 2;
+    constexpr int EH = E / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    const int t = threadIdx.x;
+    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
+    const C* src = a.in + row * N;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = src[in_pos<N, E, 0>(e, t)];
+    RowAcc<C> acc{sm};
+    fft_pencil<N, E, +1>(v, acc, t, a.twN);
+    const R sc = (R)a.scale;
+    C* dst = a.out + row * N;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        v[e] = cscale(v[e], sc);
+        dst[out_pos<N, E>(e, t)] = v[e];
+    }
+    if constexpr (MODE == XI_R2C) {
+        // stage the real source in smem (as R[N] over the same buffer)
+        R* rs = reinterpret_cast<R*>(sm);
+        __syncthreads();
+        const R pr = (R)a.pref, rm = (R)a.rho_mean;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int p = out_pos<N, E>(e, t);
+            const R rho = v[e].x * v[e].x + v[e].y * v[e].y;
+            rs[p] = pr * (rho - rm);
+        }
+        __syncthreads();
+        C z[EH];
+#pragma unroll
+        for (int e = 0; e < EH; ++e) {
+            const int q = in_pos<M, EH, 0>(e, t);
+            z[e] = mk<C>(rs[2 * q], rs[2 * q + 1]);
+        }
+        fft_pencil<M, EH, -1>(z, acc, t, a.twM);
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
+        __syncthreads();
+        r2c_post_store<N, R>(acc, t, a.vh + row * M, a.twN);
+    }
+}
+
+enum XR2CSrc { XR_DENSITY = 0, XR_REAL = 1 };
+
+// r2c along x of a real source: the density pref(|psi|^2 - rho_mean) of psi
+// (XR_DENSITY) or a real array Vin (XR_REAL), into the packed vh rows.
+template <int N, typename R, int SRC>
+__global__ void k_x_r2c(XArgs<R> a) {
+    using C = cx_t<R>;
+    constexpr int E = qx_row_efull(N);
+    constexpr int M = N / 2;
+    constexpr int EH = E / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    const int t = threadIdx.x;
+    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
+    C z[EH];
+    const R pr = (R)a.pref, rm = (R)a.rho_mean;
+#pragma unroll
+    for (int e = 0; e < EH; ++e) {
+        const int q = in_pos<M, EH, 0>(e, t);
+        if constexpr (SRC == XR_DENSITY) {
+            const C p0 = a.in[row * N + 2 * q], p1 = a.in[row * N + 2 * q + 1];
+            z[e] = mk<C>(pr * (p0.x * p0.x + p0.y * p0.y - rm), pr * (p1.x * p1.x + p1.y * p1.y - rm));
+        } else {
+            const C pair = reinterpret_cast<const C*>(a.Vin + row * N)[q];
+            z[e] = pair;
+        }
+    }
+    RowAcc<C> acc{sm};
+    fft_pencil<M, EH, -1>(z, acc, t, a.twM);
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
+    __syncthreads();
+    r2c_post_store<N, R>(acc, t, a.vh + row * M, a.twN);
+}
+
+enum XC2RFlags {
+    XC_WRITE_V = 1,    // store the potential row
+    XC_KICK = 2,       // kick psi (real space) by the potential
+    XC_WRITE_PSI = 4,  // store the kicked psi in real space
+    XC_FWD = 8,        // forward x FFT of the kicked psi -> out
+};
+
+// c2r along x of the packed vh rows -> V (unnormalised, FFTW convention);
+// then optionally kick psi by V (dt), store psi, or forward-transform it.
+template <int N, typename R, int FLAGS>
+__global__ void k_x_c2r(XArgs<R> a) {
+    using C = cx_t<R>;
+    constexpr int E = qx_row_efull(N);
+    constexpr int M = N / 2;
+    constexpr int EH = E / 2;
+    constexpr int T = qx_row_threads(N);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    const int t = threadIdx.x;
+    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
+    RowAcc<C> acc{sm};
+    const C* hrow = a.vh + row * M;
+#pragma unroll
+    for (int i = 0; i < M / T; ++i) acc(t + i * T) = hrow[t + i * T];
+    __syncthreads();
+    C z[EH];
+#pragma unroll
+    for (int e = 0; e < EH; ++e) {
+        const int k = in_pos<M, EH, 0>(e, t);
+        const C X = acc(k);
+        if (k == 0) {
+            // X[0] = Re col0, X[N/2] = Im col0
+            z[e] = mk<C>(X.x + X.y, X.x - X.y);
+        } else {
+            const C B = cconj(acc(M - k));
+            const C s = cadd(X, B), d = csub(X, B);
+            const C w = cconj(__ldg(&a.twN[k]));  // W_N^{-k}
+            const C wd = cmul(w, d);
+            z[e] = mk<C>(s.x - wd.y, s.y + wd.x);  // s + i*wd
+        }
+    }
+    fft_pencil<M, EH, +1>(z, acc, t, a.twM);
+    // z at out_pos q holds (V[2q], V[2q+1])
+    if constexpr (FLAGS & XC_WRITE_V) {
+        C* vrow = reinterpret_cast<C*>(a.Vout + row * N);
+#pragma unroll
+        for (int e = 0; e < EH; ++e) vrow[out_pos<M, EH>(e, t)] = z[e];
+    }
+    if constexpr (FLAGS & XC_KICK) {
+        C ps[E];
+#pragma unroll
+        for (int e = 0; e < EH; ++e) {
+            const int q = out_pos<M, EH>(e, t);
+            ps[2 * e] = kick1<R>(a.in[row * N + 2 * q], z[e].x, a.dt);
+            ps[2 * e + 1] = kick1<R>(a.in[row * N + 2 * q + 1], z[e].y, a.dt);
+        }
+        if constexpr (FLAGS & XC_WRITE_PSI) {
+#pragma unroll
+            for (int e = 0; e < EH; ++e) {
+                const int q = out_pos<M, EH>(e, t);
+                a.out[row * N + 2 * q] = ps[2 * e];
+                a.out[row * N + 2 * q + 1] = ps[2 * e + 1];
+            }
+        }
+        if constexpr (FLAGS & XC_FWD) {
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < EH; ++e) {
+                const int q = out_pos<M, EH>(e, t);
+                acc(2 * q) = ps[2 * e];
+                acc(2 * q + 1) = ps[2 * e + 1];
+            }
+            __syncthreads();
+            C v[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+            fft_pencil<N, E, -1>(v, acc, t, a.twN);
+            C* dst = a.out + row * N;
+#pragma unroll
+            for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// strided passes.  Array A of shape [outer][N][X] (y pass) or, for the last
+// axis, [N][rows][X] (3D, pencil along z with rows = N y-rows) / [N][X] (2D).
+// Tile: G groups x TX columns x N; blockDim = (TX, T, G), T = N / E.
+// Dynamic smem: G * N * pitch C with pitch = TX (+1 if TX*sizeof(C) < 128).
+// ---------------------------------------------------------------------------
+
+__host__ __device__ constexpr int qx_col_e(int N) { return qx_lcm_radices(N) < 8 && N >= 8 ? 8 : qx_lcm_radices(N); }
+
+template <typename R> struct SArgs {
+    cx_t<R>* a;
+    const cx_t<R>* tw;   // exp(-2 pi i j/N)
+    int X;               // columns of the array (N or N/2)
+    int dim;
+    int N;
+    double phase_fac;    // drift: -dt/2 * dk^2  (phase = fac * |n|^2)
+    double scale;        // drift: 1/S
+    double pois_c;       // Poisson: -1/(dk^2 S) (times 1/|n|^2)
+    double pois_g0;      // Poisson multiplier of the k = 0 mode
+    double* partial;     // per-block reduction output (kinetic)
+};
+
+template <typename C> __device__ __forceinline__ int col_pitch(int TX) {
+    return TX * (int)sizeof(C) < 128 ? TX + 1 : TX;
+}
+
+// y pass (3D): pencils along y of an [outer][N][X] array; blockIdx = (x tile, outer)
+template <int N, typename R, int SIGN>
+__global__ void k_y_pass(SArgs<R> s) {
+    using C = cx_t<R>;
+    constexpr int E = qx_col_e(N);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int TX = blockDim.x;
+    const int c = threadIdx.x, t = threadIdx.y;
+    const int pitch = col_pitch<C>(TX);
+    C* sm = reinterpret_cast<C*>(smem_raw) + c;
+    ColAcc<C> acc{sm, pitch};
+    const long base = (long)blockIdx.y * N * s.X + (long)blockIdx.x * TX + c;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)in_pos<N, E, 0>(e, t) * s.X];
+    fft_pencil<N, E, SIGN>(v, acc, t, s.tw);
+#pragma unroll
+    for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * s.X] = v[e];
+}
+
+enum LAOp { LA_FWD = 0, LA_INV = 1, LA_DRIFT = 2, LA_POISSON = 3, LA_KIN = 4 };
+
+// Poisson multiplier of integer |n|^2 (src/field.cxx:250-256,279-285)
+template <typename R> __device__ __forceinline__ R pois_mult(long M2, const SArgs<R>& s);
+template <> __device__ __forceinline__ float pois_mult<float>(long M2, const SArgs<float>& s) {
+    return M2 == 0 ? (float)s.pois_g0 : (float)s.pois_c * __frcp_rn((float)M2);
+}
+template <> __device__ __forceinline__ double pois_mult<double>(long M2, const SArgs<double>& s) {
+    return M2 == 0 ? s.pois_g0 : s.pois_c / (double)M2;
+}
+
+// Last-axis pass.  3D: pencils along z of [N][N][X]; blockIdx = (x tile,
+// y group); G = 1: y = blockIdx.y; G = 2: rows {g, N-g} (g = 0 pairs 0 with
+// N/2) so the mirror -k_y of every row is in the block.  2D: pencils along y
+// of [N][X]; blockIdx = (x tile).
+template <int N, typename R, int OP>
+__global__ void k_la_pass(SArgs<R> s) {
+    using C = cx_t<R>;
+    constexpr int E = qx_col_e(N);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int TX = blockDim.x, G = blockDim.z;
+    const int c = threadIdx.x, t = threadIdx.y, g = threadIdx.z;
+    const int pitch = col_pitch<C>(TX);
+    C* sm0 = reinterpret_cast<C*>(smem_raw);
+    ColAcc<C> acc{sm0 + (long)g * N * pitch + c, pitch};
+    const int x0 = blockIdx.x * TX;
+    const int x = x0 + c;
+    int y = 0;
+    long base, pstride;
+    if (s.dim == 3) {
+        const int gi = blockIdx.y;
+        if (G == 1) y = gi;
+        else y = (g == 0) ? gi : (gi == 0 ? N / 2 : N - gi);
+        base = (long)y * s.X + x;
+        pstride = (long)N * s.X;
+    } else {
+        base = x;
+        pstride = s.X;
+    }
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)in_pos<N, E, 0>(e, t) * pstride];
+    if constexpr (OP == LA_INV) {
+        fft_pencil<N, E, +1>(v, acc, t, s.tw);
+    } else {
+        fft_pencil<N, E, -1>(v, acc, t, s.tw);
+    }
+    if constexpr (OP == LA_FWD || OP == LA_INV) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];
+        return;
+    }
+    // |n|^2 contribution of x (and y in 3D)
+    const int nx = (s.X == N) ? signed_mode(x, N) : x;  // half arrays: x < N/2
+    const int ny = (s.dim == 3) ? signed_mode(y, N) : 0;
+    const long mxy = (long)nx * nx + (long)ny * ny;
+    if constexpr (OP == LA_KIN) {
+        double acc_k = 0.0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int nz = signed_mode(out_pos<N, E>(e, t), N);
+            const double m2 = (double)(mxy + (long)nz * nz);
+            acc_k += m2 * ((double)v[e].x * (double)v[e].x + (double)v[e].y * (double)v[e].y);
+        }
+        __shared__ double red[32];
+        const double tot = block_reduce<0>(acc_k, red);
+        if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
+            s.partial[blockIdx.x + (long)gridDim.x * blockIdx.y] = tot;
+        return;
+    }
+    if constexpr (OP == LA_DRIFT) {
+        const R sc = (R)s.scale;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int nz = signed_mode(out_pos<N, E>(e, t), N);
+            const long m2 = mxy + (long)nz * nz;
+            v[e] = cscale(cmul(v[e], cis<R>(s.phase_fac * (double)m2)), sc);
+        }
+    }
+    if constexpr (OP == LA_POISSON) {
+        if (x0 == 0) {
+            // stage the forward result so column 0 can read its mirror mode
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+            __syncthreads();
+            if (c == 0) {
+                const int gm = (s.dim == 3 && G == 2) ? ((y == 0 || y == N / 2) ? g : 1 - g) : g;
+                ColAcc<C> macc{sm0 + (long)gm * N * pitch, pitch};
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int p = out_pos<N, E>(e, t);
+                    const int nz = signed_mode(p, N);
+                    const long mA = (long)ny * ny + (long)nz * nz;
+                    const long mB = mA + (long)(N / 2) * (N / 2);
+                    const R gA = pois_mult<R>(mA, s), gB = pois_mult<R>(mB, s);
+                    const R al = R(0.5) * (gA + gB), be = R(0.5) * (gA - gB);
+                    const C cm = cconj(macc((N - p) % N));
+                    v[e] = cadd(cscale(v[e], al), cscale(cm, be));
+                }
+            }
+        }
+        if (!(x0 == 0 && c == 0)) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int nz = signed_mode(out_pos<N, E>(e, t), N);
+                v[e] = cscale(v[e], pois_mult<R>(mxy + (long)nz * nz, s));
+            }
+        }
+    }
+    // back to stage-0 input order, then the inverse transform
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+    fft_pencil<N, E, +1>(v, acc, t, s.tw);
+#pragma unroll
+    for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];
+}
+
+}  // namespace qx

@@ -1,0 +1,45 @@
+// qx_ops.hpp -- host-side launchers of the pass kernels (no CUDA templates
+// exposed).  One instantiation per precision lives in qx_ops_f32.cu /
+// qx_ops_f64.cu.  All launches go to the caller's stream; nothing allocates.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace qx {
+
+// supported grid sizes N (per axis)
+bool supported_n(int N);
+
+enum XC2R { C2R_WRITE_V = 1, C2R_KICK = 2, C2R_WRITE_PSI = 4, C2R_FWD = 8 };
+enum LaOp { OP_FWD = 0, OP_INV = 1, OP_DRIFT = 2, OP_POISSON = 3, OP_KIN = 4 };
+
+// Launch geometry knobs (autotuned per (N, dim, precision); 0 = default).
+struct Tune {
+    int x_rows = 0;   // rows per block in x passes
+    int y_tx = 0;     // columns per tile in y passes
+    int la_tx = 0;    // columns per tile in last-axis passes
+};
+
+template <typename R> struct Ops {
+    using C = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
+    struct XP {
+        const C* in; C* out; C* vh; const R* Vin; R* Vout;
+        const C* twN; const C* twM;
+        long rows; double dt, pref, rho_mean, scale;
+    };
+    struct SP {
+        C* a; const C* tw; int X, dim, N;
+        double phase_fac, scale, pois_c, pois_g0; double* partial;
+    };
+    static void x_fwd(int N, const XP& a, bool kick, const Tune& tu, cudaStream_t st);
+    static void x_inv(int N, const XP& a, bool r2c, const Tune& tu, cudaStream_t st);
+    static void x_r2c(int N, const XP& a, bool real_src, const Tune& tu, cudaStream_t st);
+    static void x_c2r(int N, const XP& a, int flags, const Tune& tu, cudaStream_t st);
+    // y pass of an [outer][N][X] array (3D only)
+    static void y_pass(int N, int outer, const SP& s, int sign, const Tune& tu, cudaStream_t st);
+    // last-axis pass; returns the number of blocks (partials written for OP_KIN)
+    static long la_pass(int N, const SP& s, int op, const Tune& tu, cudaStream_t st);
+    static long la_blocks(int N, int X, int dim, int op, const Tune& tu);
+};
+
+}  // namespace qx
