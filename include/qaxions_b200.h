@@ -137,6 +137,24 @@ int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx);
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 int qx_sync(qx_field_t *h);
 
+/* Allocation-free density statistics of a psi array in the CALLER's device
+ * memory (no counterpart in the reference).  For callers that may not allocate
+ * device memory while they run: an application whose own pool or caching
+ * allocator owns the device memory, a time loop that cannot take the implicit
+ * synchronisation of cudaMalloc/cudaFree, a fixed memory budget.  Computes
+ * out[0] = sum |psi|^2, out[1] = max |psi|^2, out[2] = out[1] / (out[0]/sites)
+ * (the rhomax of Field::computeEnergy, src/field.cxx:216-226) into `out`, 3
+ * doubles of device memory, asynchronously on `stream` (a cudaStream_t, NULL
+ * for the default stream).  psi: `sites` complex values (dtype QX_C128 double2
+ * or QX_C64 float2) on the current device.  Scratch is a fixed per-device array
+ * inside the library sized for at most QX_NOALLOC_MAX_SITES sites; larger
+ * sizes are rejected.  The first call on a device looks up that array's device
+ * address -- make it before any stream capture.  Calls that overlap on the GPU
+ * share the scratch and race.  Errors: qx_noalloc_last_error(). */
+#define QX_NOALLOC_MAX_SITES 134217728LL /* 512^3 */
+int qx_rho_stats_noalloc(const void *psi, long long sites, int dtype, double *out, void *stream);
+const char *qx_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
