@@ -132,8 +132,10 @@ int qx_time_steps(qx_field_t *h, int nsteps, int use_graph, float *ms);
 /* per-pass average device time of the fused loop body over nsteps bodies;
  * names: max_entries x 64 chars.  Advances the state. */
 int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, double *ms, int *n_out);
-/* launch geometry overrides (0 = default) */
-int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx);
+/* launch geometry overrides (0 = default): rows per x-pass block, tile columns
+ * of y / last-axis passes, strided-pass kernel family (1 = TMA-fed persistent,
+ * 0 = direct loads; -1 = keep), TMA ring depth */
+int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf);
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 int qx_sync(qx_field_t *h);
 

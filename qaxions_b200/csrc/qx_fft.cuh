@@ -47,8 +47,10 @@ template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
 }
 
 // ---------------------------------------------------------------------------
-// Radix plans (compile time).  L = 2^e: [2^(e%3) if e%3] + [8]*(e/3) (e <= 3:
-// one stage of radix L).  L = 3*2^k: [4]*(k/2) + [2]*(k%2) + [3].
+// Radix plans (compile time).  L = 2^e: [8]*(e/3) + [2^(e%3) if e%3] (e <= 3:
+// one stage of radix L) -- the radix-8 stages come first so that every
+// shared-memory exchange of a one-warp-per-row transform is bank-conflict free
+// under RowAcc's padding.  L = 3*2^k: [4]*(k/2) + [2]*(k%2) + [3].
 // ---------------------------------------------------------------------------
 
 __host__ __device__ constexpr bool qx_is_pow2(int L) { return L > 0 && (L & (L - 1)) == 0; }
@@ -64,7 +66,7 @@ __host__ __device__ constexpr int qx_radix(int L, int s) {
         const int e = qx_log2(L);
         if (e <= 3) return L;
         const int rem = e % 3;
-        if (rem) return s == 0 ? (1 << rem) : 8;
+        if (rem) return s == e / 3 ? (1 << rem) : 8;
         return 8;
     }
     const int k = qx_log2(L / 3);
@@ -187,7 +189,7 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const C* 
                 constexpr int stw = L / (Ns * r);
 #pragma unroll
                 for (int m = 1; m < r; ++m) {
-                    C w = __ldg(&tw[k * m * stw]);
+                    C w = tw[k * m * stw];  // global (read-only path) or a shared-memory copy
                     if (SIGN > 0) w.y = -w.y;
                     v[b * r + m] = cmul(v[b * r + m], w);
                 }

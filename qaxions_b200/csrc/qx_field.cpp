@@ -161,8 +161,10 @@ static typename Ops<R>::XP xp0(const Geometry& g, const typename Ops<R>::C* twN,
 }
 
 template <typename R>
-static typename Ops<R>::SP sp0(const Geometry& g, typename Ops<R>::C* a, const typename Ops<R>::C* tw, int X) {
+static typename Ops<R>::SP sp0(int* err, const Geometry& g, typename Ops<R>::C* a, const typename Ops<R>::C* tw,
+                               int X) {
     typename Ops<R>::SP s{};
+    s.err = err;
     s.a = a;
     s.tw = tw;
     s.X = X;
@@ -178,8 +180,8 @@ template <typename R> void B200FFTBackend<R>::forward_c2c(void* data) {
     a.in = d;
     a.out = d;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, d, twN_, g_.N), -1, *tune_, st_);
-    Ops<R>::la_pass(g_.N, sp0<R>(g_, d, twN_, g_.N), OP_FWD, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, twN_, g_.N), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, twN_, g_.N), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C* out) {
@@ -187,13 +189,13 @@ template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C
     a.in = in;
     a.out = out;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, out, twN_, g_.N), -1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,out, twN_, g_.N), -1, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2c(void* data) {
     C* d = static_cast<C*>(data);
-    Ops<R>::la_pass(g_.N, sp0<R>(g_, d, twN_, g_.N), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, d, twN_, g_.N), +1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, twN_, g_.N), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, twN_, g_.N), +1, *tune_, st_);
     auto a = xp0<R>(g_, twN_, twM_);
     a.in = d;
     a.out = d;
@@ -206,14 +208,14 @@ template <typename R> void B200FFTBackend<R>::forward_r2c(void* in_real, void* o
     a.Vin = static_cast<const R*>(in_real);
     a.vh = h;
     Ops<R>::x_r2c(g_.N, a, true, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, h, twN_, g_.N / 2), -1, *tune_, st_);
-    Ops<R>::la_pass(g_.N, sp0<R>(g_, h, twN_, g_.N / 2), OP_FWD, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2r(void* in_half, void* out_real) {
     C* h = static_cast<C*>(in_half);
-    Ops<R>::la_pass(g_.N, sp0<R>(g_, h, twN_, g_.N / 2), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(g_, h, twN_, g_.N / 2), +1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), +1, *tune_, st_);
     auto a = xp0<R>(g_, twN_, twM_);
     a.vh = h;
     a.Vout = static_cast<R*>(out_real);
@@ -270,6 +272,9 @@ class FieldT final : public Field {
         vh_.alloc(sizeof(C) * g_.hsites);
         red_.alloc(sizeof(double) * 2 * kRedBlocks);
         redout_.alloc(sizeof(double) * 4);
+        errbuf_.alloc(sizeof(int));
+        err_ = errbuf_.as<int>();
+        QX_CUDA(cudaMemsetAsync(errbuf_.p, 0, sizeof(int), st_));
         auto tN = twiddles<C>(cfg.N), tM = twiddles<C>(cfg.N / 2);
         twN_.alloc(sizeof(C) * tN.size());
         twM_.alloc(sizeof(C) * tM.size());
@@ -278,7 +283,7 @@ class FieldT final : public Field {
         QX_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
-        fft_ = std::make_unique<B200FFTBackend<R>>(g_, twN_.as<C>(), twM_.as<C>(), &tune_, st_);
+        fft_ = std::make_unique<B200FFTBackend<R>>(g_, twN_.as<C>(), twM_.as<C>(), &tune_, st_, err_);
         QX_CUDA(cudaStreamSynchronize(st_));
     }
 
@@ -299,7 +304,7 @@ class FieldT final : public Field {
     C* vh() { return vh_.as<C>(); }
 
     typename Ops<R>::XP xp() { return xp0<R>(g_, twN_.as<C>(), twM_.as<C>()); }
-    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(g_, a, twN_.as<C>(), X); }
+    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(err_, g_,a, twN_.as<C>(), X); }
 
     // ---- pass sequences ----
     void y_fwd(C* a, int X) {
@@ -448,6 +453,7 @@ class FieldT final : public Field {
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
         graph_exec_ = nullptr;
     }
+    void invalidate_graph() override { drop_graph(); }
 
     // ---- reductions ----
     std::vector<double> reduce(int kind) {
@@ -482,10 +488,10 @@ class FieldT final : public Field {
         mpsi_.alloc(sizeof(C) * g_.S);
         fft_->forward_c2c_partial(psi(), mpsi_.as<C>());
         auto s = sp(mpsi_.as<C>(), g_.N);
-        const long nblk = Ops<R>::la_blocks(g_.N, g_.N, g_.dim, OP_KIN, tune_);
-        kin_.alloc(sizeof(double) * (nblk + 1));
+        const long cap = Ops<R>::la_blocks(g_.N, g_.N, g_.dim, OP_KIN, tune_);
+        kin_.alloc(sizeof(double) * (cap + 1));
         s.partial = kin_.as<double>();
-        Ops<R>::la_pass(g_.N, s, OP_KIN, tune_, st_);
+        const long nblk = Ops<R>::la_pass(g_.N, s, OP_KIN, tune_, st_);
         Misc<R>::fold_sum(kin_.as<double>(), nblk, redout_.as<double>(), st_);
         double ks = 0.0;
         QX_CUDA(cudaMemcpyAsync(&ks, redout_.p, sizeof(double), cudaMemcpyDeviceToHost, st_));
@@ -766,6 +772,7 @@ class FieldT final : public Field {
         step(nsteps);
         QX_CUDA(cudaEventRecord(e1, st_));
         QX_CUDA(cudaEventSynchronize(e1));
+        check_device_error();
         float ms = 0.f;
         QX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         cudaEventDestroy(e0);
@@ -841,11 +848,26 @@ class FieldT final : public Field {
 
     void* psi_device() override { return psi_.p; }
     void* V_device() override { return V_.p; }
-    void sync() override { QX_CUDA(cudaStreamSynchronize(st_)); }
+    void sync() override {
+        QX_CUDA(cudaStreamSynchronize(st_));
+        check_device_error();
+    }
+
+    // A pass kernel whose bounded wait for a tile load timed out raised the
+    // flag and returned early; report it (and clear it) as an error.
+    void check_device_error() {
+        int h = 0;
+        QX_CUDA(cudaMemcpy(&h, errbuf_.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            QX_CUDA(cudaMemset(errbuf_.p, 0, sizeof(int)));
+            throw std::runtime_error("a pass kernel timed out waiting for a tile load; results are invalid");
+        }
+    }
 
   private:
     int device_ = 0;
-    DevBuf psi_, V_, vh_, twN_, twM_, red_, redout_;
+    DevBuf psi_, V_, vh_, twN_, twM_, red_, redout_, errbuf_;
+    int* err_ = nullptr;
     DevBuf mpsi_, mvh_, kin_, specP_, specC_, stage_;
     std::map<long, std::unique_ptr<DevBuf>> bintab_;
     std::unique_ptr<B200FFTBackend<R>> fft_;

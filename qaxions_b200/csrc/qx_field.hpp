@@ -68,8 +68,8 @@ template <typename R>
 class B200FFTBackend : public FFTBackend {
   public:
     using C = typename Ops<R>::C;
-    B200FFTBackend(const Geometry& g, const C* twN, const C* twM, const Tune* tune, cudaStream_t st)
-        : g_(g), twN_(twN), twM_(twM), tune_(tune), st_(st) {}
+    B200FFTBackend(const Geometry& g, const C* twN, const C* twM, const Tune* tune, cudaStream_t st, int* err)
+        : g_(g), twN_(twN), twM_(twM), tune_(tune), st_(st), err_(err) {}
     void forward_c2c(void* data) override;
     void backward_c2c(void* data) override;
     void forward_r2c(void* in_real, void* out_half) override;
@@ -87,6 +87,7 @@ class B200FFTBackend : public FFTBackend {
     const C* twM_;
     const Tune* tune_;
     cudaStream_t st_;
+    int* err_;  // device flag raised by a timed-out wait in a pass kernel
 };
 
 class Field {
@@ -158,6 +159,8 @@ class Field {
     double dt() const { return ds_; }
     void set_dt(double dt) { ds_ = dt; }
     Tune& tune() { return tune_; }
+    // drop the captured loop-body graph (after launch geometry changes)
+    virtual void invalidate_graph() = 0;
 
   protected:
     FieldConfig cfg_;

@@ -32,12 +32,23 @@ namespace qx {
 // ---------------------------------------------------------------------------
 
 // contiguous row, one padding element per 8 (bank-conflict-free stride-8 and
-// stride-64 exchanges for 8- and 16-byte elements)
+// stride-64 exchanges for 8- and 16-byte elements).  A row's threads all sit
+// in one warp (qx_row_threads(N) divides 32), so its exchanges only need a
+// warp barrier; `mask` names the warp's existing lanes (partial last warp).
 template <typename C> struct RowAcc {
     C* base;
+    unsigned mask;
     __device__ __forceinline__ C& operator()(int p) const { return base[p + (p >> 3)]; }
-    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
 };
+
+// lanes of the calling thread's warp that exist in this block
+__device__ __forceinline__ unsigned warp_lanes_mask() {
+    const int n = blockDim.x * blockDim.y * blockDim.z;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int left = n - (tid & ~31);
+    return left >= 32 ? 0xffffffffu : ((1u << left) - 1u);
+}
 __host__ __device__ constexpr int row_smem_elems(int n) { return n + (n >> 3) + 1; }
 
 // column of a strided tile: element p of this pencil at base[p * pitch]
@@ -68,6 +79,16 @@ template <> __device__ __forceinline__ double2 cis<double>(double phi) {
     double s, c;
     sincos(reduce_2pi(phi), &s, &c);
     return make_double2(c, s);
+}
+
+// exp(i phi) in FP64 with the argument reduced mod 2 pi
+__device__ __forceinline__ double2 cis_d(double phi) {
+    double s, c;
+    sincos(reduce_2pi(phi), &s, &c);
+    return make_double2(c, s);
+}
+__device__ __forceinline__ double2 dcmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 
 // psi * exp(-i dt V)   (src/field.cxx:100-112)
@@ -146,7 +167,7 @@ __global__ void k_x_fwd(XArgs<R> a) {
         v[e] = src[p];
         if constexpr (MODE == XF_KICK) v[e] = kick1<R>(v[e], a.Vin[row * N + p], a.dt);
     }
-    RowAcc<C> acc{sm};
+    RowAcc<C> acc{sm, warp_lanes_mask()};
     fft_pencil<N, E, -1>(v, acc, t, a.twN);
     C* dst = a.out + row * N;
 #pragma unroll
@@ -198,7 +219,7 @@ __global__ void k_x_inv(XArgs<R> a) {
     C v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = src[in_pos<N, E, 0>(e, t)];
-    RowAcc<C> acc{sm};
+    RowAcc<C> acc{sm, warp_lanes_mask()};
     fft_pencil<N, E, +1>(v, acc, t, a.twN);
     const R sc = (R)a.scale;
     C* dst = a.out + row * N;
@@ -210,7 +231,7 @@ __global__ void k_x_inv(XArgs<R> a) {
     if constexpr (MODE == XI_R2C) {
         // stage the real source in smem (as R[N] over the same buffer)
         R* rs = reinterpret_cast<R*>(sm);
-        __syncthreads();
+        acc.sync();
         const R pr = (R)a.pref, rm = (R)a.rho_mean;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -218,18 +239,17 @@ __global__ void k_x_inv(XArgs<R> a) {
             const R rho = v[e].x * v[e].x + v[e].y * v[e].y;
             rs[p] = pr * (rho - rm);
         }
-        __syncthreads();
+        acc.sync();
         C z[EH];
 #pragma unroll
         for (int e = 0; e < EH; ++e) {
-            const int q = in_pos<M, EH, 0>(e, t);
-            z[e] = mk<C>(rs[2 * q], rs[2 * q + 1]);
+            z[e] = reinterpret_cast<const C*>(rs)[in_pos<M, EH, 0>(e, t)];  // (rho[2q], rho[2q+1])
         }
         fft_pencil<M, EH, -1>(z, acc, t, a.twM);
-        __syncthreads();
+        acc.sync();
 #pragma unroll
         for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
-        __syncthreads();
+        acc.sync();
         r2c_post_store<N, R>(acc, t, a.vh + row * M, a.twN);
     }
 }
@@ -261,12 +281,12 @@ __global__ void k_x_r2c(XArgs<R> a) {
             z[e] = pair;
         }
     }
-    RowAcc<C> acc{sm};
+    RowAcc<C> acc{sm, warp_lanes_mask()};
     fft_pencil<M, EH, -1>(z, acc, t, a.twM);
-    __syncthreads();
+    acc.sync();
 #pragma unroll
     for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
-    __syncthreads();
+    acc.sync();
     r2c_post_store<N, R>(acc, t, a.vh + row * M, a.twN);
 }
 
@@ -290,11 +310,11 @@ __global__ void k_x_c2r(XArgs<R> a) {
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
-    RowAcc<C> acc{sm};
+    RowAcc<C> acc{sm, warp_lanes_mask()};
     const C* hrow = a.vh + row * M;
 #pragma unroll
     for (int i = 0; i < M / T; ++i) acc(t + i * T) = hrow[t + i * T];
-    __syncthreads();
+    acc.sync();
     C z[EH];
 #pragma unroll
     for (int e = 0; e < EH; ++e) {
@@ -335,14 +355,14 @@ __global__ void k_x_c2r(XArgs<R> a) {
             }
         }
         if constexpr (FLAGS & XC_FWD) {
-            __syncthreads();
+            acc.sync();
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
                 const int q = out_pos<M, EH>(e, t);
                 acc(2 * q) = ps[2 * e];
                 acc(2 * q + 1) = ps[2 * e + 1];
             }
-            __syncthreads();
+            acc.sync();
             C v[E];
 #pragma unroll
             for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
@@ -471,12 +491,15 @@ __global__ void k_la_pass(SArgs<R> s) {
         return;
     }
     if constexpr (OP == LA_DRIFT) {
-        const R sc = (R)s.scale;
+        // exp(-i dt/2 dk^2 |n|^2)/S = A(nx, ny) B(nz), both in FP64 (same
+        // arithmetic as the TMA-fed pass, which tabulates B)
+        const double2 A = cis_d(s.phase_fac * (double)mxy);
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int nz = signed_mode(out_pos<N, E>(e, t), N);
-            const long m2 = mxy + (long)nz * nz;
-            v[e] = cscale(cmul(v[e], cis<R>(s.phase_fac * (double)m2)), sc);
+            const long nz = signed_mode(out_pos<N, E>(e, t), N);
+            const double2 b = cis_d(s.phase_fac * (double)(nz * nz));
+            const double2 w = dcmul(A, make_double2(b.x * s.scale, b.y * s.scale));
+            v[e] = cmul(v[e], mk<C>((R)w.x, (R)w.y));
         }
     }
     if constexpr (OP == LA_POISSON) {

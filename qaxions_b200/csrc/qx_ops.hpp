@@ -18,6 +18,8 @@ struct Tune {
     int x_rows = 0;   // rows per block in x passes
     int y_tx = 0;     // columns per tile in y passes
     int la_tx = 0;    // columns per tile in last-axis passes
+    int tma = 1;      // strided passes: 1 = persistent TMA-fed kernels, 0 = direct-load kernels
+    int nbuf = 0;     // TMA ring depth (0 = as many 64 KB-class tiles as fit in ~200 KB)
 };
 
 template <typename R> struct Ops {
@@ -30,6 +32,7 @@ template <typename R> struct Ops {
     struct SP {
         C* a; const C* tw; int X, dim, N;
         double phase_fac, scale, pois_c, pois_g0; double* partial;
+        int* err;  // device flag set when a bounded wait times out
     };
     static void x_fwd(int N, const XP& a, bool kick, const Tune& tu, cudaStream_t st);
     static void x_inv(int N, const XP& a, bool r2c, const Tune& tu, cudaStream_t st);

@@ -6,8 +6,11 @@
 #include <string>
 #include <type_traits>
 
+#include <cudaTypedefs.h>
+
 #include "qx_kernels.cuh"
 #include "qx_ops.hpp"
+#include "qx_tma.cuh"
 
 namespace qx {
 
@@ -140,10 +143,134 @@ static int pick_tx(int X, int T, int G, int want, size_t elem, int N, int maxthr
     return tx;
 }
 
+// ---------------------------------------------------------------------------
+// TMA-fed persistent strided passes
+// ---------------------------------------------------------------------------
+
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+            throw std::runtime_error("cuTensorMapEncodeTiled is unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// Tensor map over a complex [NZ][N][X] array viewed as reals [NZ][N][2X];
+// box = 2TX reals x `box` positions along dim 1 (pencil_dim 1) or dim 2.
+template <typename R>
+static CUtensorMap make_tmap(const void* base, int X, int N, int NZ, int TX, int box, int pencil_dim) {
+    CUtensorMap tm;
+    cuuint64_t dims[3] = {(cuuint64_t)2 * X, (cuuint64_t)N, (cuuint64_t)NZ};
+    cuuint64_t strides[2] = {(cuuint64_t)2 * X * sizeof(R), (cuuint64_t)2 * X * (cuuint64_t)N * sizeof(R)};
+    cuuint32_t boxd[3] = {(cuuint32_t)(2 * TX), (cuuint32_t)(pencil_dim == 1 ? box : 1),
+                          (cuuint32_t)(pencil_dim == 2 ? box : 1)};
+    cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = tmap_encoder()(&tm, sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                                      3, const_cast<void*>(base), dims, strides, boxd, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return tm;
+}
+
+static int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cache[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 1;
+    }
+    return cache[dev];
+}
+
+// Launch geometry of a TMA pencil pass.
+struct TmaGeom {
+    int TX, T, nbuf, box, nbox;
+    size_t tile_bytes;
+};
+
+template <int NN, typename R>
+static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
+    using C = cx_t<R>;
+    TmaGeom g;
+    g.T = NN / tma_e<NN, R>();
+    int tx = want_tx > 0 ? want_tx : (int)(128 / sizeof(C));
+    while (tx > 1 && ((X % tx) || tx * g.T > 512)) tx >>= 1;
+    g.TX = tx;
+    g.box = NN <= 256 ? NN : 256;
+    g.nbox = NN / g.box;
+    g.tile_bytes = ((size_t)NN * tx * sizeof(C) + 1023) & ~(size_t)1023;  // 1 KB-aligned buffer stride
+    if (sizeof(R) == 4 && tx < 2) throw std::logic_error("TMA tile narrower than 16 bytes");
+    // ring depth: as many tiles as fit beside the tables in ~210 KB
+    const size_t tables = tma_smem_bytes<R>(NN, tx, 0, op);
+    int nb = tu.nbuf > 0 ? tu.nbuf : (int)((210 * 1024 - tables) / g.tile_bytes);
+    g.nbuf = nb < 2 ? 2 : (nb > 4 ? 4 : nb);
+    return g;
+}
+
+// Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
+template <int NN, typename R, int OP>
+static long launch_tma(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
+                       const Tune& tu, cudaStream_t st) {
+    const TmaGeom g = tma_geom<NN, R>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
+    TArgs<R> s;
+    s.tw = a.tw;
+    s.X = a.X;
+    s.N = NN;
+    s.outer = outer;
+    s.pencil_dim = pencil_dim;
+    s.la3d = la3d;
+    s.TX = g.TX;
+    s.tiles_x = a.X / g.TX;
+    s.nbuf = g.nbuf;
+    s.nbox = g.nbox;
+    s.box = g.box;
+    s.n_tiles = (long)s.tiles_x * outer;
+    s.phase_fac = a.phase_fac;
+    s.scale = a.scale;
+    s.pois_c = a.pois_c;
+    s.pois_g0 = a.pois_g0;
+    s.col0_external = col0_ext;
+    s.partial = a.partial;
+    s.err = a.err;
+    const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim);
+    auto kern = k_pencil_tma<NN, R, OP>;
+    const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP);
+    set_smem(kern, smem);
+    static int bps_cache[64] = {0};
+    const int key = g.nbuf * 8 + (g.TX == 16 ? 4 : g.TX == 8 ? 3 : g.TX == 4 ? 2 : g.TX == 2 ? 1 : 0);
+    int& bps = bps_cache[key & 63];
+    if (!bps) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, g.TX * g.T, smem) != cudaSuccess || bps < 1)
+            bps = 1;
+    }
+    long grid = (long)sm_count() * bps;
+    if (grid > s.n_tiles) grid = s.n_tiles;
+    dim3 blk(g.TX, g.T, 1);
+    kern<<<(unsigned)grid, blk, smem, st>>>(tm, s);
+    QX_LAUNCH_CHECK();
+    return grid;
+}
+
 template <typename R>
 void Ops<R>::y_pass(int N, int outer, const SP& a, int sign, const Tune& tu, cudaStream_t st) {
     using C = cx_t<R>;
     const SArgs<R> s = to_s<R>(a);
+    if (tu.tma) {
+        QX_FOR_N(N, {
+            if (sign < 0) launch_tma<NN, R, OP_FWD>(a, outer, outer, 1, 0, 0, tu, st);
+            else launch_tma<NN, R, OP_INV>(a, outer, outer, 1, 0, 0, tu, st);
+        });
+        return;
+    }
     QX_FOR_N(N, {
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;
@@ -183,6 +310,7 @@ static int la_max_threads(int op) {
 template <typename R>
 long Ops<R>::la_blocks(int N, int X, int dim, int op, const Tune& tu) {
     using C = cx_t<R>;
+    if (tu.tma) return (long)sm_count() * 32;  // upper bound of the persistent grid
     QX_FOR_N(N, {
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;
@@ -194,10 +322,38 @@ long Ops<R>::la_blocks(int N, int X, int dim, int op, const Tune& tu) {
     return 0;
 }
 
+template <int NN, typename R>
+static void launch_col0(const typename Ops<R>::SP& a, cudaStream_t st) {
+    using C = cx_t<R>;
+    constexpr int E0 = qx_lcm_radices(NN);
+    dim3 blk(2, NN / E0, 1);
+    k_poisson_col0<NN, R><<<NN / 2, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.pois_c, a.pois_g0);
+    QX_LAUNCH_CHECK();
+}
+
 template <typename R>
 long Ops<R>::la_pass(int N, const SP& a, int op, const Tune& tu, cudaStream_t st) {
     using C = cx_t<R>;
     const SArgs<R> s = to_s<R>(a);
+    if (tu.tma) {
+        QX_FOR_N(N, {
+            const int d3 = a.dim == 3 ? 1 : 0;
+            const int NZ = d3 ? NN : 1, outer = d3 ? NN : 1, pdim = d3 ? 2 : 1;
+            long grid = 0;
+            switch (op) {
+                case OP_FWD: grid = launch_tma<NN, R, OP_FWD>(a, NZ, outer, pdim, d3, 0, tu, st); break;
+                case OP_INV: grid = launch_tma<NN, R, OP_INV>(a, NZ, outer, pdim, d3, 0, tu, st); break;
+                case OP_DRIFT: grid = launch_tma<NN, R, OP_DRIFT>(a, NZ, outer, pdim, d3, 0, tu, st); break;
+                case OP_POISSON:
+                    grid = launch_tma<NN, R, OP_POISSON>(a, NZ, outer, pdim, d3, d3, tu, st);
+                    if (d3) launch_col0<NN, R>(a, st);
+                    break;
+                case OP_KIN: grid = launch_tma<NN, R, OP_KIN>(a, NZ, outer, pdim, d3, 0, tu, st); break;
+                default: throw std::invalid_argument("la_pass: bad op");
+            }
+            return grid;
+        });
+    }
     QX_FOR_N(N, {
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;

@@ -1,0 +1,367 @@
+// qx_tma.cuh -- TMA-fed persistent pencil passes (sm_100a).
+//
+// A strided pass streams tiles of TX columns x N pencil positions through a
+// ring of NBUF shared-memory buffers.  One elected thread moves every tile with
+// the Tensor Memory Accelerator: a tensor load (cp.async.bulk.tensor, completion
+// counted on one mbarrier per buffer) brings the tile in, all threads run the
+// pencil FFT in place in the tile, and a tensor store (bulk group) writes the
+// finished tile back from the same buffer.  The buffer of tile k-1 is refilled
+// with tile k+NBUF-1 once its store has been read out, so loads, the FFT and
+// stores of neighbouring tiles overlap and the threads issue no global
+// loads/stores of their own.
+//
+// Twiddles (and, for the drift pass, the z-dependent phase factors) are staged
+// in shared memory once per launch.  The drift phase exp(-i dt/2 dk^2 |n|^2)/S
+// is factored exactly as A(nx, ny) * B(nz); both factors are evaluated in FP64
+// with the argument reduced mod 2 pi, multiplied in FP64 and rounded once.
+//
+// Every mbarrier wait is bounded (~1 s of SM clock); on time-out the kernel
+// sets *err, waits (bounded) for its own loads still in flight and for its
+// stores, and returns.  No clusters, no multicast: a block only loads what it
+// transforms.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qx_kernels.cuh"
+#include "qx_ops.hpp"
+
+namespace qx {
+
+// ---------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: gives up after `limit` SM cycles (default 2^31, ~1 s)
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit = (1LL << 31)) {
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (clock64() - t0 > limit) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* tm, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* tm, int c0, int c1, int c2, uint32_t src) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
+        ::"l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(src)
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// wait until at most one bulk group still reads its shared-memory source
+__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
+// persistent TMA pencil pass
+// ---------------------------------------------------------------------------
+
+// elements per thread of a strided pass
+template <int N, typename R> __host__ __device__ constexpr int tma_e() {
+    return (N >= 256 && sizeof(R) == 4) ? 16 : qx_lcm_radices(N);
+}
+
+__host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
+
+// dynamic shared memory of a pass: NBUF tiles + twiddles + drift factors
+// (drift only) + column-0 stash (Poisson only) + 1 KB base-alignment slack
+template <typename R> __host__ __device__ constexpr size_t tma_smem_bytes(int N, int TX, int nbuf, int op) {
+    return (size_t)nbuf * align1k((size_t)N * TX * 2 * sizeof(R)) + (size_t)N * 2 * sizeof(R) +
+           (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) + 1024;
+}
+
+template <typename R> struct TArgs {
+    const cx_t<R>* tw;   // exp(-2 pi i j/N), global
+    int X;               // columns (N for psi, N/2 for the packed half spectrum)
+    int N;
+    int outer;           // tiles along the non-pencil axis (z for y passes, y for z passes, 1 in 2D)
+    int pencil_dim;      // 1: pencil along tensor dim 1 (y passes, 2D last axis); 2: along dim 2 (3D z)
+    int la3d;            // last-axis pass of a 3D array (pencil = z, outer = y)
+    int TX, tiles_x, nbuf, nbox, box;
+    long n_tiles;
+    double phase_fac, scale, pois_c, pois_g0;
+    int col0_external;   // 3D Poisson: column 0 is finished by k_poisson_col0
+    double* partial;     // OP_KIN per-block sums
+    int* err;            // set to 1 when a wait timed out
+};
+
+template <int N, typename R, int OP>
+__global__ void __launch_bounds__(512, 1) k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
+    using C = cx_t<R>;
+    constexpr int E = tma_e<N, R>();
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[8];
+    __shared__ int s_ok;
+    __shared__ double red[32];
+    const int TX = s.TX;
+    const int c = threadIdx.x, t = threadIdx.y;
+    const int tid = c + TX * t;
+    const int nthr = TX * blockDim.y;
+    const uint32_t tile_bytes = (uint32_t)((size_t)N * TX * sizeof(C));
+    const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
+    C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    C* tws = bufs + s.nbuf * tile_elems;
+    double2* bz = reinterpret_cast<double2*>(tws + N);
+    C* col0 = reinterpret_cast<C*>(bz + (OP == OP_DRIFT ? N : 0));
+
+    auto coords = [&](long id, int j, int& c0, int& c1, int& c2) {
+        const int x0 = (int)(id % s.tiles_x) * TX;
+        const int o = (int)(id / s.tiles_x);
+        c0 = 2 * x0;
+        if (s.pencil_dim == 1) { c1 = j * s.box; c2 = o; }
+        else { c1 = o; c2 = j * s.box; }
+    };
+    auto issue_load = [&](long id, int b) {
+        const uint32_t bar = smem_u32(&mbar[b]);
+        mbar_expect_tx(bar, tile_bytes);
+        for (int j = 0; j < s.nbox; ++j) {
+            int c0, c1, c2;
+            coords(id, j, c0, c1, c2);
+            tma_load_3d(smem_u32(bufs + b * tile_elems + (long)j * s.box * TX), &tm, c0, c1, c2, bar);
+        }
+    };
+
+    // per-launch tables and barriers
+    for (int i = tid; i < N; i += nthr) tws[i] = s.tw[i];
+    if constexpr (OP == OP_DRIFT) {
+        for (int i = tid; i < N; i += nthr) {
+            const long n = signed_mode(i, N);
+            const double2 w = cis_d(s.phase_fac * (double)(n * n));
+            bz[i] = make_double2(w.x * s.scale, w.y * s.scale);
+        }
+    }
+    if (tid == 0) {
+        for (int b = 0; b < s.nbuf; ++b) mbar_init(smem_u32(&mbar[b]), 1);
+        fence_mbar_init();
+        for (int k = 0; k < s.nbuf - 1; ++k) {
+            const long id = blockIdx.x + (long)k * gridDim.x;
+            if (id < s.n_tiles) issue_load(id, k);
+        }
+    }
+    __syncthreads();
+
+    double kin = 0.0;
+    for (int k = 0;; ++k) {
+        const long id = blockIdx.x + (long)k * gridDim.x;
+        if (id >= s.n_tiles) break;
+        const int b = k % s.nbuf;
+        const uint32_t parity = (uint32_t)((k / s.nbuf) & 1);
+        if (tid == 0) s_ok = mbar_wait_bounded(smem_u32(&mbar[b]), parity) ? 1 : 0;
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) {
+                atomicExch(s.err, 1);
+                for (int j = 1; j < s.nbuf - 1; ++j) {  // this block's other loads in flight
+                    const long jd = id + (long)j * gridDim.x;
+                    if (jd < s.n_tiles)
+                        mbar_wait_bounded(smem_u32(&mbar[(k + j) % s.nbuf]), (uint32_t)(((k + j) / s.nbuf) & 1),
+                                          1LL << 28);
+                }
+                bulk_wait_all();
+            }
+            __syncthreads();
+            return;
+        }
+        (void)mbar_try(smem_u32(&mbar[b]), parity);  // acquire the TMA writes in every thread
+        C* tile = bufs + b * tile_elems;
+        const int x0 = (int)(id % s.tiles_x) * TX;
+        const int o = (int)(id / s.tiles_x);
+        const int x = x0 + c;
+        ColAcc<C> acc{tile + c, TX};
+        C v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+        if constexpr (OP == OP_INV) fft_pencil<N, E, +1>(v, acc, t, tws);
+        else fft_pencil<N, E, -1>(v, acc, t, tws);
+
+        bool store = true;
+        if constexpr (OP == OP_KIN) {
+            const int nx = (s.X == N) ? signed_mode(x, N) : x;
+            const int ny = s.la3d ? signed_mode(o, N) : 0;
+            const long mxy = (long)nx * nx + (long)ny * ny;
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int nz = signed_mode(out_pos<N, E>(e, t), N);
+                kin += (double)(mxy + (long)nz * nz) * ((double)v[e].x * (double)v[e].x + (double)v[e].y * (double)v[e].y);
+            }
+            store = false;
+        } else if constexpr (OP == OP_DRIFT || OP == OP_POISSON) {
+            const int nx = (s.X == N) ? signed_mode(x, N) : x;
+            const int ny = s.la3d ? signed_mode(o, N) : 0;
+            const long mxy = (long)nx * nx + (long)ny * ny;
+            const bool c0ext = (OP == OP_POISSON) && s.col0_external && x0 == 0 && c == 0;
+            if constexpr (OP == OP_DRIFT) {
+                const double2 A = cis_d(s.phase_fac * (double)mxy);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const double2 w = dcmul(A, bz[out_pos<N, E>(e, t)]);
+                    v[e] = cmul(v[e], mk<C>((R)w.x, (R)w.y));
+                }
+            } else {
+                SArgs<R> sa;
+                sa.pois_c = s.pois_c;
+                sa.pois_g0 = s.pois_g0;
+                if (c0ext) {
+                    // 3D: column 0 (kx = 0 and N/2 packed) is paired with its mirror
+                    // row by k_poisson_col0; keep the forward result for it
+#pragma unroll
+                    for (int e = 0; e < E; ++e) col0[out_pos<N, E>(e, t)] = v[e];
+                } else if (x0 == 0 && !s.col0_external) {
+                    // 2D: the mirror -k_y of column 0 lies in the same pencil
+                    __syncthreads();
+#pragma unroll
+                    for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+                    __syncthreads();
+                    if (c == 0) {
+#pragma unroll
+                        for (int e = 0; e < E; ++e) {
+                            const int p = out_pos<N, E>(e, t);
+                            const long np = signed_mode(p, N);
+                            const long mA = np * np, mB = mA + (long)(N / 2) * (N / 2);
+                            const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
+                            const C cm = cconj(acc((N - p) % N));
+                            v[e] = cadd(cscale(v[e], R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
+                        }
+                    }
+                }
+                if (!(x0 == 0 && c == 0)) {
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        const int nz = signed_mode(out_pos<N, E>(e, t), N);
+                        v[e] = cscale(v[e], pois_mult<R>(mxy + (long)nz * nz, sa));
+                    }
+                }
+            }
+            // back to stage-0 order and inverse transform
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+            fft_pencil<N, E, +1>(v, acc, t, tws);
+            if (c0ext) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) v[e] = col0[out_pos<N, E>(e, t)];
+            }
+        }
+
+        if (store) {
+            // finished tile -> buffer (natural order) -> tensor store
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+            fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                for (int j = 0; j < s.nbox; ++j) {
+                    int c0, c1, c2;
+                    coords(id, j, c0, c1, c2);
+                    tma_store_3d(&tm, c0, c1, c2, smem_u32(tile + (long)j * s.box * TX));
+                }
+                bulk_commit();
+            }
+        } else {
+            __syncthreads();
+        }
+        // refill the buffer of tile k-1 (its store has been read out) with tile k+NBUF-1
+        if (tid == 0) {
+            const long nid = id + (long)(s.nbuf - 1) * gridDim.x;
+            if (nid < s.n_tiles) {
+                bulk_wait_read_1();
+                fence_proxy_async();
+                issue_load(nid, (k + s.nbuf - 1) % s.nbuf);
+            }
+        }
+    }
+    if (tid == 0) bulk_wait_all();
+    if constexpr (OP == OP_KIN) {
+        const double tot = block_reduce<0>(kin, red);
+        if (tid == 0) s.partial[blockIdx.x] = tot;
+    }
+}
+
+// 3D Poisson, column 0: rows y and N-y (0 pairs with N/2) of the packed
+// kx = {0, N/2} column, already transformed along x, y and z, get
+// C'(k) = a C(k) + b conj C(-k) with a, b from the kx = 0 and kx = N/2
+// multipliers, then the inverse z transform.  blockDim = (2, N/E).
+template <int N, typename R>
+__global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, double pois_c, double pois_g0) {
+    using C = cx_t<R>;
+    constexpr int E = qx_lcm_radices(N);
+    constexpr int X = N / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    const int g = threadIdx.x, t = threadIdx.y;
+    const int gi = blockIdx.x;
+    const int ya = gi == 0 ? 0 : gi, yb = gi == 0 ? N / 2 : N - gi;
+    const int y = g == 0 ? ya : yb;
+    const int gm = (gi == 0) ? g : 1 - g;
+    ColAcc<C> acc{sm + g, 2};
+    ColAcc<C> macc{sm + gm, 2};
+    const long pstride = (long)N * X;
+    const long base = (long)y * X;
+    for (int p = t; p < N; p += blockDim.y) acc(p) = vh[base + (long)p * pstride];
+    __syncthreads();
+    SArgs<R> sa;
+    sa.pois_c = pois_c;
+    sa.pois_g0 = pois_g0;
+    const long ny = signed_mode(y, N);
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int p = in_pos<N, E, 0>(e, t);
+        const long nz = signed_mode(p, N);
+        const long mA = ny * ny + nz * nz, mB = mA + (long)X * X;
+        const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
+        const C cm = cconj(macc((N - p) % N));
+        v[e] = cadd(cscale(acc(p), R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
+    }
+    fft_pencil<N, E, +1>(v, acc, t, tw);
+#pragma unroll
+    for (int e = 0; e < E; ++e) vh[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];
+}
+
+}  // namespace qx
