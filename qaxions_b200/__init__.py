@@ -74,7 +74,7 @@ _SIGS = {
     "qx_ic_config": ([_vp, _i, C.c_ulonglong, _i, _d, _d, _d, _d, _d, _d], _i),
     "qx_time_steps": ([_vp, _i, _i, _fp], _i),
     "qx_profile_step": ([_vp, _i, _i, C.c_char_p, _dp, _ip], _i),
-    "qx_set_tune": ([_vp, _i, _i, _i, _i, _i], _i),
+    "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
 }
@@ -341,10 +341,11 @@ class Field:
         raw = names.raw
         return [(raw[64 * i:64 * i + 64].split(b"\0")[0].decode(), float(ms[i])) for i in range(n.value)]
 
-    def set_tune(self, x_rows: int = 0, y_tx: int = 0, la_tx: int = 0, tma: int = -1, nbuf: int = 0):
+    def set_tune(self, x_rows: int = 0, y_tx: int = 0, la_tx: int = 0, tma: int = -1, nbuf: int = 0, ept: int = 0):
         """Launch geometry overrides (0 = default); tma 1/0 selects the TMA-fed
-        persistent or the direct-load strided kernels (-1 keeps the current)."""
-        self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf)
+        persistent or the direct-load strided kernels (-1 keeps the current);
+        ept 8 selects the register-lean TMA pass variant."""
+        self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, ept)
 
     def device_pointers(self):
         p, v = _vp(), _vp()

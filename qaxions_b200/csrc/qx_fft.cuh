@@ -214,6 +214,14 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const C* 
     }
 }
 
+// True when a transform's output order (out_pos) equals the next transform's
+// stage-0 input order (in_pos<.,.,0>): first and last radix agree, so a
+// forward FFT can feed an inverse FFT of the same length straight from
+// registers after a pointwise multiply (no shared-memory exchange).
+template <int L> __host__ __device__ constexpr bool qx_out_is_in() {
+    return qx_radix(L, 0) == qx_radix(L, qx_nstages(L) - 1);
+}
+
 // Full transform: v in stage-0 input order on entry (see in_pos<L,E,0>),
 // natural-order outputs at out_pos<L,E> on exit.
 template <int L, int E, int SIGN, typename C, typename Acc>

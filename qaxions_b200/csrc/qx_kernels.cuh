@@ -31,14 +31,16 @@ namespace qx {
 // shared-memory accessors
 // ---------------------------------------------------------------------------
 
-// contiguous row, one padding element per 8 (bank-conflict-free stride-8 and
-// stride-64 exchanges for 8- and 16-byte elements).  A row's threads all sit
-// in one warp (qx_row_threads(N) divides 32), so its exchanges only need a
-// warp barrier; `mask` names the warp's existing lanes (partial last warp).
+// contiguous row, one padding element per 16: with radix-8-first plans every
+// Stockham exchange, the even/odd staging and contiguous reads of a row touch
+// each 4-byte bank word at most as often as a conflict-free 8-byte access does
+// (checked for the 512- and 256-point plans with a 32-lane bank model).  A
+// row's threads all sit in one warp (qx_row_threads(N) divides 32), so its
+// exchanges only need a warp barrier; `mask` names the warp's existing lanes.
 template <typename C> struct RowAcc {
     C* base;
     unsigned mask;
-    __device__ __forceinline__ C& operator()(int p) const { return base[p + (p >> 3)]; }
+    __device__ __forceinline__ C& operator()(int p) const { return base[p + (p >> 4)]; }
     __device__ __forceinline__ void sync() const { __syncwarp(mask); }
 };
 
@@ -49,7 +51,7 @@ __device__ __forceinline__ unsigned warp_lanes_mask() {
     const int left = n - (tid & ~31);
     return left >= 32 ? 0xffffffffu : ((1u << left) - 1u);
 }
-__host__ __device__ constexpr int row_smem_elems(int n) { return n + (n >> 3) + 1; }
+__host__ __device__ constexpr int row_smem_elems(int n) { return n + (n >> 4) + 1; }
 
 // column of a strided tile: element p of this pencil at base[p * pitch]
 template <typename C> struct ColAcc {
@@ -152,7 +154,7 @@ enum XFwdMode { XF_PLAIN = 0, XF_KICK = 1 };
 
 // forward c2c along x; optional kick by V first.  (Field::kick + first FFT pass)
 template <int N, typename R, int MODE>
-__global__ void k_x_fwd(XArgs<R> a) {
+__global__ void __launch_bounds__(256, 3) k_x_fwd(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -206,7 +208,7 @@ enum XInvMode { XI_PLAIN = 0, XI_R2C = 1 };
 // inverse c2c along x (psi^_x -> psi, times scale); optionally the density
 // source pref(|psi|^2 - rho_mean) and its r2c x transform into vh.
 template <int N, typename R, int MODE>
-__global__ void k_x_inv(XArgs<R> a) {
+__global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
@@ -259,7 +261,7 @@ enum XR2CSrc { XR_DENSITY = 0, XR_REAL = 1 };
 // r2c along x of a real source: the density pref(|psi|^2 - rho_mean) of psi
 // (XR_DENSITY) or a real array Vin (XR_REAL), into the packed vh rows.
 template <int N, typename R, int SRC>
-__global__ void k_x_r2c(XArgs<R> a) {
+__global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
@@ -300,7 +302,7 @@ enum XC2RFlags {
 // c2r along x of the packed vh rows -> V (unnormalised, FFTW convention);
 // then optionally kick psi by V (dt), store psi, or forward-transform it.
 template <int N, typename R, int FLAGS>
-__global__ void k_x_c2r(XArgs<R> a) {
+__global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
@@ -533,13 +535,16 @@ __global__ void k_la_pass(SArgs<R> s) {
             }
         }
     }
-    // back to stage-0 input order, then the inverse transform
-    __syncthreads();
+    // back to stage-0 input order (a no-op when the plan's first and last
+    // radix agree), then the inverse transform
+    if constexpr (!qx_out_is_in<N>()) {
+        __syncthreads();
 #pragma unroll
-    for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
-    __syncthreads();
+        for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+        __syncthreads();
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+        for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+    }
     fft_pencil<N, E, +1>(v, acc, t, s.tw);
 #pragma unroll
     for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];

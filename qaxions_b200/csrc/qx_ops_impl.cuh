@@ -198,29 +198,34 @@ struct TmaGeom {
 };
 
 template <int NN, typename R>
-static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
+static TmaGeom tma_geom(int X, int want_tx, int op, int E, const Tune& tu) {
     using C = cx_t<R>;
     TmaGeom g;
-    g.T = NN / tma_e<NN, R>();
-    int tx = want_tx > 0 ? want_tx : (int)(128 / sizeof(C));
+    g.T = NN / E;
+    // default tile: 8 columns (64-byte rows for c64, 128-byte rows for c128) and
+    // a 3-deep ring, which lets two FP32 blocks share an SM (measured best at
+    // 512^3 against 16 columns / deeper rings)
+    int tx = want_tx > 0 ? want_tx : 8;
     while (tx > 1 && ((X % tx) || tx * g.T > 512)) tx >>= 1;
     g.TX = tx;
     g.box = NN <= 256 ? NN : 256;
     g.nbox = NN / g.box;
     g.tile_bytes = ((size_t)NN * tx * sizeof(C) + 1023) & ~(size_t)1023;  // 1 KB-aligned buffer stride
     if (sizeof(R) == 4 && tx < 2) throw std::logic_error("TMA tile narrower than 16 bytes");
-    // ring depth: as many tiles as fit beside the tables in ~210 KB
+    // ring depth: 3, or as many tiles as fit beside the tables in ~210 KB
     const size_t tables = tma_smem_bytes<R>(NN, tx, 0, op);
     int nb = tu.nbuf > 0 ? tu.nbuf : (int)((210 * 1024 - tables) / g.tile_bytes);
+    if (tu.nbuf == 0 && nb > 3) nb = 3;
     g.nbuf = nb < 2 ? 2 : (nb > 4 ? 4 : nb);
     return g;
 }
 
 // Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
-template <int NN, typename R, int OP>
-static long launch_tma(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
-                       const Tune& tu, cudaStream_t st) {
-    const TmaGeom g = tma_geom<NN, R>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
+template <int NN, typename R, int OP, int EPT>
+static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
+                         const Tune& tu, cudaStream_t st) {
+    const TmaGeom g = tma_geom<NN, R>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP,
+                                      tma_eff_e<NN, R, EPT>(), tu);
     TArgs<R> s;
     s.tw = a.tw;
     s.X = a.X;
@@ -242,7 +247,7 @@ static long launch_tma(const typename Ops<R>::SP& a, int NZ, int outer, int penc
     s.partial = a.partial;
     s.err = a.err;
     const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim);
-    auto kern = k_pencil_tma<NN, R, OP>;
+    auto kern = k_pencil_tma<NN, R, OP, EPT>;
     const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
@@ -258,6 +263,15 @@ static long launch_tma(const typename Ops<R>::SP& a, int NZ, int outer, int penc
     kern<<<(unsigned)grid, blk, smem, st>>>(tm, s);
     QX_LAUNCH_CHECK();
     return grid;
+}
+
+// tu.ept = 8 selects the register-lean variant (8 values per thread, two
+// blocks per SM) where it is valid; otherwise the default layout
+template <int NN, typename R, int OP>
+static long launch_tma(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
+                       const Tune& tu, cudaStream_t st) {
+    if (tu.ept == 8) return launch_tma_e<NN, R, OP, 8>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    return launch_tma_e<NN, R, OP, 0>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
 }
 
 template <typename R>

@@ -127,10 +127,21 @@ template <typename R> struct TArgs {
     int* err;            // set to 1 when a wait timed out
 };
 
-template <int N, typename R, int OP>
-__global__ void __launch_bounds__(512, 1) k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
+// elements per thread actually used: EPT when it is a valid choice for N
+// (a multiple of every radix, at most N), else the default
+template <int N, typename R, int EPT> __host__ __device__ constexpr int tma_eff_e() {
+    return (EPT > 0 && EPT % qx_lcm_radices(N) == 0 && EPT <= N) ? EPT : tma_e<N, R>();
+}
+// FP32 tiles with <= 8 values per thread fit two 512-thread blocks per SM
+template <int N, typename R, int EPT> __host__ __device__ constexpr int tma_min_blocks() {
+    return (sizeof(R) == 4 && tma_eff_e<N, R, EPT>() <= 8) ? 2 : 1;
+}
+
+template <int N, typename R, int OP, int EPT>
+__global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
+    k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
-    constexpr int E = tma_e<N, R>();
+    constexpr int E = tma_eff_e<N, R, EPT>();
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[8];
     __shared__ int s_ok;
@@ -274,13 +285,16 @@ __global__ void __launch_bounds__(512, 1) k_pencil_tma(const __grid_constant__ C
                     }
                 }
             }
-            // back to stage-0 order and inverse transform
-            __syncthreads();
+            // back to stage-0 order (a no-op when the plan's first and last
+            // radix agree) and inverse transform
+            if constexpr (!qx_out_is_in<N>()) {
+                __syncthreads();
 #pragma unroll
-            for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
-            __syncthreads();
+                for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+                __syncthreads();
 #pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+                for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+            }
             fft_pencil<N, E, +1>(v, acc, t, tws);
             if (c0ext) {
 #pragma unroll
