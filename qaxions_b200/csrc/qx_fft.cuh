@@ -97,8 +97,20 @@ __host__ __device__ constexpr int qx_row_threads(int N) { return N / qx_row_eful
 
 template <typename R> struct Consts {
     static constexpr R rsqrt2 = R(0.70710678118654752440084436210484903928);
+    // rsqrt2 - R(rsqrt2): with it, x * (rsqrt2 + rsqrt2_lo) has an unbiased
+    // magnitude (|(1 +- i) h| = 1 to O(eps^2)) instead of 1 - 1.7e-8 in FP32,
+    // a bias every radix-8 stage would otherwise apply to the same modes at
+    // every time step
+    static constexpr R rsqrt2_lo = R(0.70710678118654752440084436210484903928L - (long double)R(0.70710678118654752440084436210484903928L));
     static constexpr R sqrt3_2 = R(0.86602540378443864676372317075293618347);
 };
+
+// x * 1/sqrt(2) with the constant carried to twice the working precision
+template <typename C> __device__ __forceinline__ C cscale_rsqrt2(C a) {
+    using R = decltype(C::x);
+    return mk<C>(fma(a.x, Consts<R>::rsqrt2, a.x * Consts<R>::rsqrt2_lo),
+                 fma(a.y, Consts<R>::rsqrt2, a.y * Consts<R>::rsqrt2_lo));
+}
 
 template <int SIGN, typename C> __device__ __forceinline__ void dft2(C* a) {
     C t = a[0];
@@ -132,12 +144,11 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* a) {
     C o[4] = {a[1], a[3], a[5], a[7]};
     dft4<SIGN>(e);
     dft4<SIGN>(o);
-    const R h = Consts<R>::rsqrt2;
     // o[q] *= W8^q (sign SIGN): W8^1 = h(1 + SIGN i), W8^2 = SIGN i, W8^3 = h(-1 + SIGN i)
     const C o1 = o[1], o3 = o[3];
-    o[1] = cscale(cadd(o1, cmul_si<SIGN>(o1)), h);
+    o[1] = cscale_rsqrt2(cadd(o1, cmul_si<SIGN>(o1)));
     o[2] = cmul_si<SIGN>(o[2]);
-    o[3] = cscale(csub(cmul_si<SIGN>(o3), o3), h);
+    o[3] = cscale_rsqrt2(csub(cmul_si<SIGN>(o3), o3));
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         a[q] = cadd(e[q], o[q]);
@@ -172,8 +183,35 @@ template <int L, int E> __device__ __forceinline__ int out_pos(int e, int t) {
     return t + (e / r) * T + (e % r) * (L / r);
 }
 
-template <int L, int E, int SIGN, int s, typename C, typename Acc>
-__device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const C* __restrict__ tw) {
+// Twiddle sources: a table of exp(-2 pi i j/L) (global or a shared-memory
+// copy), or a double-float pair of tables hi + lo (lo = exact - hi), which
+// applies each twiddle to twice the working precision.  A twiddle table is
+// applied with the same values at every time step, so its rounding error
+// would otherwise compound over the steps for modes whose forward and
+// inverse transforms do not cancel it (those with a drift phase).
+template <typename C> struct TwPair {
+    const C* hi;
+    const C* lo;
+};
+
+template <int SIGN, typename C> __device__ __forceinline__ C tw_mul(C v, const C* tw, int i) {
+    C w = tw[i];
+    if (SIGN > 0) w.y = -w.y;
+    return cmul(v, w);
+}
+template <int SIGN, typename C> __device__ __forceinline__ C tw_mul(C v, const TwPair<C>& tw, int i) {
+    C w = tw.hi[i], l = tw.lo[i];
+    if (SIGN > 0) {
+        w.y = -w.y;
+        l.y = -l.y;
+    }
+    const auto cx = v.x * l.x - v.y * l.y;
+    const auto cy = v.x * l.y + v.y * l.x;
+    return mk<C>(fma(v.x, w.x, fma(-v.y, w.y, cx)), fma(v.x, w.y, fma(v.y, w.x, cy)));
+}
+
+template <int L, int E, int SIGN, int s, typename C, typename Acc, typename TW>
+__device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const TW& tw) {
     constexpr int S = qx_nstages(L);
     if constexpr (s < S) {
         constexpr int r = qx_radix(L, s);
@@ -188,11 +226,7 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const C* 
                 const int k = j % Ns;
                 constexpr int stw = L / (Ns * r);
 #pragma unroll
-                for (int m = 1; m < r; ++m) {
-                    C w = tw[k * m * stw];  // global (read-only path) or a shared-memory copy
-                    if (SIGN > 0) w.y = -w.y;
-                    v[b * r + m] = cmul(v[b * r + m], w);
-                }
+                for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<SIGN>(v[b * r + m], tw, k * m * stw);
             }
             dft<r, SIGN>(&v[b * r]);
         }
@@ -214,19 +248,78 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const C* 
     }
 }
 
-// True when a transform's output order (out_pos) equals the next transform's
-// stage-0 input order (in_pos<.,.,0>): first and last radix agree, so a
-// forward FFT can feed an inverse FFT of the same length straight from
-// registers after a pointwise multiply (no shared-memory exchange).
-template <int L> __host__ __device__ constexpr bool qx_out_is_in() {
-    return qx_radix(L, 0) == qx_radix(L, qx_nstages(L) - 1);
-}
-
 // Full transform: v in stage-0 input order on entry (see in_pos<L,E,0>),
 // natural-order outputs at out_pos<L,E> on exit.
-template <int L, int E, int SIGN, typename C, typename Acc>
-__device__ __forceinline__ void fft_pencil(C (&v)[E], Acc& acc, int t, const C* __restrict__ tw) {
+template <int L, int E, int SIGN, typename C, typename Acc, typename TW>
+__device__ __forceinline__ void fft_pencil(C (&v)[E], Acc& acc, int t, const TW& tw) {
     fft_stages<L, E, SIGN, 0>(v, acc, t, tw);
+}
+
+// Twiddle source of a transform: DF = true selects double-float twiddles in
+// the FP32 form (FP64 always uses the single table).  The wave-function
+// transforms of the time step use them: the inverse transforms below undo the
+// forward stages exactly, so a forward/phase/inverse sequence alone would not
+// accumulate the twiddles' rounding, but the kick between steps does not
+// commute with it and the rounded twiddles' magnitudes are not exactly 1, so
+// with single FP32 twiddles the phase and norm errors of psi grow linearly
+// with the number of steps.  The density/potential transforms keep single
+// twiddles: V is rebuilt from psi every step and its errors do not compound.
+template <bool DF, typename C>
+__device__ __forceinline__ auto tw_src(const C* hi, const C* lo) {
+    if constexpr (DF && sizeof(C) == 8) {
+        return TwPair<C>{hi, lo};
+    } else {
+        (void)lo;
+        return hi;
+    }
+}
+
+// Position held by v[e] in the OUTPUT order of forward stage s (where stage s
+// writes its results); for the last stage this is out_pos.
+template <int L, int E, int s> __device__ __forceinline__ int stage_out_pos(int e, int t) {
+    constexpr int r = qx_radix(L, s);
+    constexpr int Ns = qx_span(L, s);
+    constexpr int T = L / E;
+    const int j = t + (e / r) * T;
+    return (j / Ns) * Ns * r + (j % Ns) + (e % r) * Ns;
+}
+
+// Undo forward stage s (inverse butterfly, then conjugate twiddles), then
+// move on to stage s-1.  Entry: v in stage_out_pos<s> order; exit of the
+// whole chain: v in stage-0 input order (in_pos<L,E,0>).
+template <int L, int E, int s, typename C, typename Acc, typename TW>
+__device__ __forceinline__ void ifft_rev_stages(C (&v)[E], Acc& acc, int t, const TW& tw) {
+    constexpr int r = qx_radix(L, s);
+    constexpr int Ns = qx_span(L, s);
+    constexpr int T = L / E;
+    constexpr int nb = E / r;
+#pragma unroll
+    for (int b = 0; b < nb; ++b) {
+        dft<r, +1>(&v[b * r]);
+        if constexpr (Ns > 1) {
+            const int k = (t + b * T) % Ns;
+            constexpr int stw = L / (Ns * r);
+#pragma unroll
+            for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<+1>(v[b * r + m], tw, k * m * stw);
+        }
+    }
+    if constexpr (s > 0) {
+        acc.sync();
+#pragma unroll
+        for (int e = 0; e < E; ++e) acc(in_pos<L, E, s>(e, t)) = v[e];
+        acc.sync();
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = acc(stage_out_pos<L, E, s - 1>(e, t));
+        ifft_rev_stages<L, E, s - 1>(v, acc, t, tw);
+    }
+}
+
+// Unnormalised inverse transform (x L) that exactly undoes fft_pencil<L,E,-1>:
+// v in natural output order (out_pos<L,E>) on entry, in stage-0 input order
+// (in_pos<L,E,0>, lane-contiguous natural order) on exit.
+template <int L, int E, typename C, typename Acc, typename TW>
+__device__ __forceinline__ void ifft_pencil_rev(C (&v)[E], Acc& acc, int t, const TW& tw) {
+    ifft_rev_stages<L, E, qx_nstages(L) - 1>(v, acc, t, tw);
 }
 
 }  // namespace qx

@@ -53,15 +53,63 @@ struct DevBuf {
 // host helpers: twiddles, packing, spectrum tables
 // ---------------------------------------------------------------------------
 
+// Twiddles exp(-2 pi i j / L).  In FP32 each value is picked among the
+// neighbours (+-2 ulp per component) of the correctly rounded pair to make
+// |w|^2 as close to 1 as possible (angle error kept within 1.5 ulp): a
+// forward/inverse transform pair cancels a twiddle's angle error but not its
+// magnitude error, and the same table is applied every time step, so a
+// magnitude bias would accumulate linearly with the number of steps.
 template <typename C> static std::vector<C> twiddles(int L) {
+    using R = decltype(C::x);
     std::vector<C> t(L);
     const long double tp = 6.283185307179586476925286766559005768L;
     for (int j = 0; j < L; ++j) {
         const long double a = -tp * (long double)j / (long double)L;
-        t[j].x = (decltype(t[j].x))cosl(a);
-        t[j].y = (decltype(t[j].y))sinl(a);
+        const long double c = cosl(a), s = sinl(a);
+        R bc = (R)c, bs = (R)s;
+        if constexpr (sizeof(R) == 4) {
+            const long double ulp = 1.0L / (1 << 24);
+            long double best = fabsl((long double)bc * bc + (long double)bs * bs - 1.0L);
+            for (int dc = -2; dc <= 2; ++dc) {
+                for (int ds = -2; ds <= 2; ++ds) {
+                    R cc = bc, ss = bs;
+                    for (int k = 0; k < (dc < 0 ? -dc : dc); ++k) cc = nextafterf(cc, dc < 0 ? -2.0f : 2.0f);
+                    for (int k = 0; k < (ds < 0 ? -ds : ds); ++k) ss = nextafterf(ss, ds < 0 ? -2.0f : 2.0f);
+                    // angle error of the candidate, in units of 2^-24
+                    const long double ang = fabsl(atan2l((long double)ss, (long double)cc) - atan2l(s, c));
+                    const long double ang_w = (ang > 3.0L) ? fabsl(ang - tp) : ang;  // across +-pi
+                    if (ang_w > 1.5L * ulp) continue;
+                    const long double m = fabsl((long double)cc * cc + (long double)ss * ss - 1.0L);
+                    if (m < best) {
+                        best = m;
+                        t[j].x = cc;
+                        t[j].y = ss;
+                    }
+                }
+            }
+            if (best == fabsl((long double)bc * bc + (long double)bs * bs - 1.0L)) {
+                t[j].x = bc;
+                t[j].y = bs;
+            }
+        } else {
+            t[j].x = bc;
+            t[j].y = bs;
+        }
     }
     return t;
+}
+
+// low parts exact - hi of a twiddle table (zero for FP64, which does not use them)
+template <typename C> static std::vector<C> twiddles_lo(int L, const std::vector<C>& hi) {
+    using R = decltype(C::x);
+    std::vector<C> lo(L);
+    const long double tp = 6.283185307179586476925286766559005768L;
+    for (int j = 0; j < L; ++j) {
+        const long double a = -tp * (long double)j / (long double)L;
+        lo[j].x = sizeof(R) == 4 ? (R)(cosl(a) - (long double)hi[j].x) : (R)0;
+        lo[j].y = sizeof(R) == 4 ? (R)(sinl(a) - (long double)hi[j].y) : (R)0;
+    }
+    return lo;
 }
 
 static inline long mirror_row(int dim, int N, long r) {
@@ -149,10 +197,12 @@ std::vector<double> spectrum_k_axis(int N, int mode, int nbins, double L) {
 // ---------------------------------------------------------------------------
 
 template <typename R>
-static typename Ops<R>::XP xp0(const Geometry& g, const typename Ops<R>::C* twN, const typename Ops<R>::C* twM) {
+static typename Ops<R>::XP xp0(const Geometry& g, const TwTables<typename Ops<R>::C>& tw) {
     typename Ops<R>::XP a{};
-    a.twN = twN;
-    a.twM = twM;
+    a.twN = tw.N;
+    a.twM = tw.M;
+    a.twN_lo = tw.N_lo;
+    a.twM_lo = tw.M_lo;
     a.rows = g.rows;
     a.scale = 1.0;
     a.pref = 1.0;
@@ -161,12 +211,15 @@ static typename Ops<R>::XP xp0(const Geometry& g, const typename Ops<R>::C* twN,
 }
 
 template <typename R>
-static typename Ops<R>::SP sp0(int* err, const Geometry& g, typename Ops<R>::C* a, const typename Ops<R>::C* tw,
-                               int X) {
+static typename Ops<R>::SP sp0(int* err, const Geometry& g, typename Ops<R>::C* a,
+                               const TwTables<typename Ops<R>::C>& tw, int X) {
     typename Ops<R>::SP s{};
     s.err = err;
     s.a = a;
-    s.tw = tw;
+    s.tw = tw.N;
+    // double-float twiddles for wave-function arrays (X = N) only: the
+    // half-spectrum (density / potential) transforms keep single twiddles
+    s.tw_lo = X == g.N ? tw.N_lo : nullptr;
     s.X = X;
     s.dim = g.dim;
     s.N = g.N;
@@ -176,27 +229,27 @@ static typename Ops<R>::SP sp0(int* err, const Geometry& g, typename Ops<R>::C* 
 
 template <typename R> void B200FFTBackend<R>::forward_c2c(void* data) {
     C* d = static_cast<C*>(data);
-    auto a = xp0<R>(g_, twN_, twM_);
+    auto a = xp0<R>(g_, tw_);
     a.in = d;
     a.out = d;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, twN_, g_.N), -1, *tune_, st_);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, twN_, g_.N), OP_FWD, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, tw_, g_.N), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, tw_, g_.N), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C* out) {
-    auto a = xp0<R>(g_, twN_, twM_);
+    auto a = xp0<R>(g_, tw_);
     a.in = in;
     a.out = out;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,out, twN_, g_.N), -1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,out, tw_, g_.N), -1, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2c(void* data) {
     C* d = static_cast<C*>(data);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, twN_, g_.N), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, twN_, g_.N), +1, *tune_, st_);
-    auto a = xp0<R>(g_, twN_, twM_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, tw_, g_.N), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, tw_, g_.N), +1, *tune_, st_);
+    auto a = xp0<R>(g_, tw_);
     a.in = d;
     a.out = d;
     Ops<R>::x_inv(g_.N, a, false, *tune_, st_);
@@ -204,19 +257,19 @@ template <typename R> void B200FFTBackend<R>::backward_c2c(void* data) {
 
 template <typename R> void B200FFTBackend<R>::forward_r2c(void* in_real, void* out_half) {
     C* h = static_cast<C*>(out_half);
-    auto a = xp0<R>(g_, twN_, twM_);
+    auto a = xp0<R>(g_, tw_);
     a.Vin = static_cast<const R*>(in_real);
     a.vh = h;
     Ops<R>::x_r2c(g_.N, a, true, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), -1, *tune_, st_);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), OP_FWD, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2r(void* in_half, void* out_real) {
     C* h = static_cast<C*>(in_half);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, twN_, g_.N / 2), +1, *tune_, st_);
-    auto a = xp0<R>(g_, twN_, twM_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), +1, *tune_, st_);
+    auto a = xp0<R>(g_, tw_);
     a.vh = h;
     a.Vout = static_cast<R*>(out_real);
     Ops<R>::x_c2r(g_.N, a, C2R_WRITE_V, *tune_, st_);
@@ -276,14 +329,20 @@ class FieldT final : public Field {
         err_ = errbuf_.as<int>();
         QX_CUDA(cudaMemsetAsync(errbuf_.p, 0, sizeof(int), st_));
         auto tN = twiddles<C>(cfg.N), tM = twiddles<C>(cfg.N / 2);
+        auto tNl = twiddles_lo<C>(cfg.N, tN), tMl = twiddles_lo<C>(cfg.N / 2, tM);
         twN_.alloc(sizeof(C) * tN.size());
         twM_.alloc(sizeof(C) * tM.size());
+        twNl_.alloc(sizeof(C) * tN.size());
+        twMl_.alloc(sizeof(C) * tM.size());
         QX_CUDA(cudaMemcpy(twN_.p, tN.data(), sizeof(C) * tN.size(), cudaMemcpyHostToDevice));
         QX_CUDA(cudaMemcpy(twM_.p, tM.data(), sizeof(C) * tM.size(), cudaMemcpyHostToDevice));
+        QX_CUDA(cudaMemcpy(twNl_.p, tNl.data(), sizeof(C) * tN.size(), cudaMemcpyHostToDevice));
+        QX_CUDA(cudaMemcpy(twMl_.p, tMl.data(), sizeof(C) * tM.size(), cudaMemcpyHostToDevice));
+        tw_ = TwTables<C>{twN_.as<C>(), twM_.as<C>(), twNl_.as<C>(), twMl_.as<C>()};
         QX_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
-        fft_ = std::make_unique<B200FFTBackend<R>>(g_, twN_.as<C>(), twM_.as<C>(), &tune_, st_, err_);
+        fft_ = std::make_unique<B200FFTBackend<R>>(g_, tw_, &tune_, st_, err_);
         QX_CUDA(cudaStreamSynchronize(st_));
     }
 
@@ -303,8 +362,8 @@ class FieldT final : public Field {
     R* V() { return V_.as<R>(); }
     C* vh() { return vh_.as<C>(); }
 
-    typename Ops<R>::XP xp() { return xp0<R>(g_, twN_.as<C>(), twM_.as<C>()); }
-    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(err_, g_,a, twN_.as<C>(), X); }
+    typename Ops<R>::XP xp() { return xp0<R>(g_, tw_); }
+    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(err_, g_, a, tw_, X); }
 
     // ---- pass sequences ----
     void y_fwd(C* a, int X) {
@@ -866,7 +925,8 @@ class FieldT final : public Field {
 
   private:
     int device_ = 0;
-    DevBuf psi_, V_, vh_, twN_, twM_, red_, redout_, errbuf_;
+    DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, red_, redout_, errbuf_;
+    TwTables<C> tw_{};
     int* err_ = nullptr;
     DevBuf mpsi_, mvh_, kin_, specP_, specC_, stage_;
     std::map<long, std::unique_ptr<DevBuf>> bintab_;

@@ -64,12 +64,21 @@ struct Geometry {
     long fftw_ksites() const { return rows * (N / 2 + 1); }
 };
 
+// device twiddle tables exp(-2 pi i j/L) for L = N and N/2, with the low
+// parts (exact - table) used by the FP32 form's double-float twiddles
+template <typename C> struct TwTables {
+    const C* N;
+    const C* M;
+    const C* N_lo;
+    const C* M_lo;
+};
+
 template <typename R>
 class B200FFTBackend : public FFTBackend {
   public:
     using C = typename Ops<R>::C;
-    B200FFTBackend(const Geometry& g, const C* twN, const C* twM, const Tune* tune, cudaStream_t st, int* err)
-        : g_(g), twN_(twN), twM_(twM), tune_(tune), st_(st), err_(err) {}
+    B200FFTBackend(const Geometry& g, const TwTables<C>& tw, const Tune* tune, cudaStream_t st, int* err)
+        : g_(g), tw_(tw), tune_(tune), st_(st), err_(err) {}
     void forward_c2c(void* data) override;
     void backward_c2c(void* data) override;
     void forward_r2c(void* in_real, void* out_half) override;
@@ -83,8 +92,7 @@ class B200FFTBackend : public FFTBackend {
 
   private:
     Geometry g_;
-    const C* twN_;
-    const C* twM_;
+    TwTables<C> tw_;
     const Tune* tune_;
     cudaStream_t st_;
     int* err_;  // device flag raised by a timed-out wait in a pass kernel

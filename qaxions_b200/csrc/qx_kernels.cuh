@@ -93,6 +93,15 @@ __device__ __forceinline__ double2 dcmul(double2 a, double2 b) {
     return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 
+// v * w with w in FP64 and one rounding of the product.  A unit factor that is
+// applied every step with the same value (the drift phase of each mode) must
+// not be rounded to FP32 first: its fixed rounding error would compound
+// linearly over the steps instead of averaging out.
+template <typename C> __device__ __forceinline__ C cmul_d(C v, double2 w) {
+    const double vx = v.x, vy = v.y;
+    return mk<C>((decltype(C::x))fma(vx, w.x, -vy * w.y), (decltype(C::x))fma(vx, w.y, vy * w.x));
+}
+
 // psi * exp(-i dt V)   (src/field.cxx:100-112)
 template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, double dt) {
     return cmul(p, cis<R>(-dt * (double)v));
@@ -144,6 +153,8 @@ template <typename R> struct XArgs {
     R* Vout;                // real rows of N
     const cx_t<R>* twN;     // exp(-2 pi i j/N), j < N
     const cx_t<R>* twM;     // exp(-2 pi i j/(N/2)), j < N/2
+    const cx_t<R>* twN_lo;  // exact - twN (double-float twiddles of the FP32 form)
+    const cx_t<R>* twM_lo;
     long rows;
     double dt;              // kick time step
     double pref, rho_mean;  // r2c source pref*(|psi|^2 - rho_mean)
@@ -157,7 +168,7 @@ template <int N, typename R, int MODE>
 __global__ void __launch_bounds__(256, 3) k_x_fwd(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -170,7 +181,7 @@ __global__ void __launch_bounds__(256, 3) k_x_fwd(XArgs<R> a) {
         if constexpr (MODE == XF_KICK) v[e] = kick1<R>(v[e], a.Vin[row * N + p], a.dt);
     }
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    fft_pencil<N, E, -1>(v, acc, t, a.twN);
+    fft_pencil<N, E, -1>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
     C* dst = a.out + row * N;
 #pragma unroll
     for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
@@ -213,22 +224,22 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
     const C* src = a.in + row * N;
     C v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = src[in_pos<N, E, 0>(e, t)];
+    for (int e = 0; e < E; ++e) v[e] = src[out_pos<N, E>(e, t)];
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    fft_pencil<N, E, +1>(v, acc, t, a.twN);
+    ifft_pencil_rev<N, E>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
     const R sc = (R)a.scale;
     C* dst = a.out + row * N;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
         v[e] = cscale(v[e], sc);
-        dst[out_pos<N, E>(e, t)] = v[e];
+        dst[in_pos<N, E, 0>(e, t)] = v[e];
     }
     if constexpr (MODE == XI_R2C) {
         // stage the real source in smem (as R[N] over the same buffer)
@@ -237,7 +248,7 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
         const R pr = (R)a.pref, rm = (R)a.rho_mean;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int p = out_pos<N, E>(e, t);
+            const int p = in_pos<N, E, 0>(e, t);
             const R rho = v[e].x * v[e].x + v[e].y * v[e].y;
             rs[p] = pr * (rho - rm);
         }
@@ -247,7 +258,7 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
         for (int e = 0; e < EH; ++e) {
             z[e] = reinterpret_cast<const C*>(rs)[in_pos<M, EH, 0>(e, t)];  // (rho[2q], rho[2q+1])
         }
-        fft_pencil<M, EH, -1>(z, acc, t, a.twM);
+        fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
         acc.sync();
 #pragma unroll
         for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
@@ -266,7 +277,7 @@ __global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
         }
     }
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    fft_pencil<M, EH, -1>(z, acc, t, a.twM);
+    fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
     acc.sync();
 #pragma unroll
     for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
@@ -308,7 +319,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
     constexpr int T = qx_row_threads(N);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -320,7 +331,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     C z[EH];
 #pragma unroll
     for (int e = 0; e < EH; ++e) {
-        const int k = in_pos<M, EH, 0>(e, t);
+        const int k = out_pos<M, EH>(e, t);
         const C X = acc(k);
         if (k == 0) {
             // X[0] = Re col0, X[N/2] = Im col0
@@ -333,25 +344,25 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
             z[e] = mk<C>(s.x - wd.y, s.y + wd.x);  // s + i*wd
         }
     }
-    fft_pencil<M, EH, +1>(z, acc, t, a.twM);
-    // z at out_pos q holds (V[2q], V[2q+1])
+    ifft_pencil_rev<M, EH>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
+    // z at in_pos<M, EH, 0> q holds (V[2q], V[2q+1])
     if constexpr (FLAGS & XC_WRITE_V) {
         C* vrow = reinterpret_cast<C*>(a.Vout + row * N);
 #pragma unroll
-        for (int e = 0; e < EH; ++e) vrow[out_pos<M, EH>(e, t)] = z[e];
+        for (int e = 0; e < EH; ++e) vrow[in_pos<M, EH, 0>(e, t)] = z[e];
     }
     if constexpr (FLAGS & XC_KICK) {
         C ps[E];
 #pragma unroll
         for (int e = 0; e < EH; ++e) {
-            const int q = out_pos<M, EH>(e, t);
+            const int q = in_pos<M, EH, 0>(e, t);
             ps[2 * e] = kick1<R>(a.in[row * N + 2 * q], z[e].x, a.dt);
             ps[2 * e + 1] = kick1<R>(a.in[row * N + 2 * q + 1], z[e].y, a.dt);
         }
         if constexpr (FLAGS & XC_WRITE_PSI) {
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
-                const int q = out_pos<M, EH>(e, t);
+                const int q = in_pos<M, EH, 0>(e, t);
                 a.out[row * N + 2 * q] = ps[2 * e];
                 a.out[row * N + 2 * q + 1] = ps[2 * e + 1];
             }
@@ -360,7 +371,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
             acc.sync();
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
-                const int q = out_pos<M, EH>(e, t);
+                const int q = in_pos<M, EH, 0>(e, t);
                 acc(2 * q) = ps[2 * e];
                 acc(2 * q + 1) = ps[2 * e + 1];
             }
@@ -368,7 +379,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
             C v[E];
 #pragma unroll
             for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
-            fft_pencil<N, E, -1>(v, acc, t, a.twN);
+            fft_pencil<N, E, -1>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
             C* dst = a.out + row * N;
 #pragma unroll
             for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
@@ -388,6 +399,7 @@ __host__ __device__ constexpr int qx_col_e(int N) { return qx_lcm_radices(N) < 8
 template <typename R> struct SArgs {
     cx_t<R>* a;
     const cx_t<R>* tw;   // exp(-2 pi i j/N)
+    const cx_t<R>* tw_lo;  // exact - tw (FP32 double-float twiddles)
     int X;               // columns of the array (N or N/2)
     int dim;
     int N;
@@ -402,12 +414,13 @@ template <typename C> __device__ __forceinline__ int col_pitch(int TX) {
     return TX * (int)sizeof(C) < 128 ? TX + 1 : TX;
 }
 
-// y pass (3D): pencils along y of an [outer][N][X] array; blockIdx = (x tile, outer)
-template <int N, typename R, int SIGN>
+// y pass (3D): pencils along y of an [outer][N][X] array; blockIdx = (x tile, outer).
+// DF: double-float twiddles (wave-function arrays of the FP32 form).
+template <int N, typename R, int SIGN, bool DF>
 __global__ void k_y_pass(SArgs<R> s) {
     using C = cx_t<R>;
     constexpr int E = qx_col_e(N);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     const int TX = blockDim.x;
     const int c = threadIdx.x, t = threadIdx.y;
     const int pitch = col_pitch<C>(TX);
@@ -415,11 +428,19 @@ __global__ void k_y_pass(SArgs<R> s) {
     ColAcc<C> acc{sm, pitch};
     const long base = (long)blockIdx.y * N * s.X + (long)blockIdx.x * TX + c;
     C v[E];
+    if constexpr (SIGN < 0) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)in_pos<N, E, 0>(e, t) * s.X];
-    fft_pencil<N, E, SIGN>(v, acc, t, s.tw);
+        for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)in_pos<N, E, 0>(e, t) * s.X];
+        fft_pencil<N, E, -1>(v, acc, t, tw_src<DF>(s.tw, s.tw_lo));
 #pragma unroll
-    for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * s.X] = v[e];
+        for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * s.X] = v[e];
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)out_pos<N, E>(e, t) * s.X];
+        ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(s.tw, s.tw_lo));
+#pragma unroll
+        for (int e = 0; e < E; ++e) s.a[base + (long)in_pos<N, E, 0>(e, t) * s.X] = v[e];
+    }
 }
 
 enum LAOp { LA_FWD = 0, LA_INV = 1, LA_DRIFT = 2, LA_POISSON = 3, LA_KIN = 4 };
@@ -436,12 +457,12 @@ template <> __device__ __forceinline__ double pois_mult<double>(long M2, const S
 // Last-axis pass.  3D: pencils along z of [N][N][X]; blockIdx = (x tile,
 // y group); G = 1: y = blockIdx.y; G = 2: rows {g, N-g} (g = 0 pairs 0 with
 // N/2) so the mirror -k_y of every row is in the block.  2D: pencils along y
-// of [N][X]; blockIdx = (x tile).
-template <int N, typename R, int OP>
+// of [N][X]; blockIdx = (x tile).  DF as for k_y_pass.
+template <int N, typename R, int OP, bool DF>
 __global__ void k_la_pass(SArgs<R> s) {
     using C = cx_t<R>;
     constexpr int E = qx_col_e(N);
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     const int TX = blockDim.x, G = blockDim.z;
     const int c = threadIdx.x, t = threadIdx.y, g = threadIdx.z;
     const int pitch = col_pitch<C>(TX);
@@ -461,17 +482,21 @@ __global__ void k_la_pass(SArgs<R> s) {
         base = x;
         pstride = s.X;
     }
+    // forward transforms load in stage-0 order and store in natural order; the
+    // inverse runs the other way round
+    auto load_pos = [&](int e) { return OP == LA_INV ? out_pos<N, E>(e, t) : in_pos<N, E, 0>(e, t); };
+    auto store_pos = [&](int e) { return OP == LA_INV ? in_pos<N, E, 0>(e, t) : out_pos<N, E>(e, t); };
     C v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)in_pos<N, E, 0>(e, t) * pstride];
+    for (int e = 0; e < E; ++e) v[e] = s.a[base + (long)load_pos(e) * pstride];
     if constexpr (OP == LA_INV) {
-        fft_pencil<N, E, +1>(v, acc, t, s.tw);
+        ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(s.tw, s.tw_lo));
     } else {
-        fft_pencil<N, E, -1>(v, acc, t, s.tw);
+        fft_pencil<N, E, -1>(v, acc, t, tw_src<DF>(s.tw, s.tw_lo));
     }
     if constexpr (OP == LA_FWD || OP == LA_INV) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];
+        for (int e = 0; e < E; ++e) s.a[base + (long)store_pos(e) * pstride] = v[e];
         return;
     }
     // |n|^2 contribution of x (and y in 3D)
@@ -501,7 +526,7 @@ __global__ void k_la_pass(SArgs<R> s) {
             const long nz = signed_mode(out_pos<N, E>(e, t), N);
             const double2 b = cis_d(s.phase_fac * (double)(nz * nz));
             const double2 w = dcmul(A, make_double2(b.x * s.scale, b.y * s.scale));
-            v[e] = cmul(v[e], mk<C>((R)w.x, (R)w.y));
+            v[e] = cmul_d(v[e], w);
         }
     }
     if constexpr (OP == LA_POISSON) {
@@ -535,19 +560,11 @@ __global__ void k_la_pass(SArgs<R> s) {
             }
         }
     }
-    // back to stage-0 input order (a no-op when the plan's first and last
-    // radix agree), then the inverse transform
-    if constexpr (!qx_out_is_in<N>()) {
-        __syncthreads();
+    // the inverse transform undoes the forward stages in reverse order straight
+    // from the forward output order and ends in the load order
+    ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(s.tw, s.tw_lo));
 #pragma unroll
-        for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
-    }
-    fft_pencil<N, E, +1>(v, acc, t, s.tw);
-#pragma unroll
-    for (int e = 0; e < E; ++e) s.a[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];
+    for (int e = 0; e < E; ++e) s.a[base + (long)in_pos<N, E, 0>(e, t) * pstride] = v[e];
 }
 
 }  // namespace qx

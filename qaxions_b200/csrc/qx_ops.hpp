@@ -28,10 +28,11 @@ template <typename R> struct Ops {
     struct XP {
         const C* in; C* out; C* vh; const R* Vin; R* Vout;
         const C* twN; const C* twM;
+        const C* twN_lo; const C* twM_lo;  // low parts (exact - table), FP32 double-float twiddles
         long rows; double dt, pref, rho_mean, scale;
     };
     struct SP {
-        C* a; const C* tw; int X, dim, N;
+        C* a; const C* tw; const C* tw_lo; int X, dim, N;
         double phase_fac, scale, pois_c, pois_g0; double* partial;
         int* err;  // device flag set when a bounded wait times out
     };

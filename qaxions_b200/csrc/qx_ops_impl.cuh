@@ -46,13 +46,14 @@ static void set_smem(K kernel, size_t bytes) {
 template <typename R> static XArgs<R> to_x(const typename Ops<R>::XP& a) {
     XArgs<R> x;
     x.in = a.in; x.out = a.out; x.vh = a.vh; x.Vin = a.Vin; x.Vout = a.Vout;
-    x.twN = a.twN; x.twM = a.twM; x.rows = a.rows; x.dt = a.dt; x.pref = a.pref;
+    x.twN = a.twN; x.twM = a.twM; x.twN_lo = a.twN_lo; x.twM_lo = a.twM_lo;
+    x.rows = a.rows; x.dt = a.dt; x.pref = a.pref;
     x.rho_mean = a.rho_mean; x.scale = a.scale;
     return x;
 }
 template <typename R> static SArgs<R> to_s(const typename Ops<R>::SP& a) {
     SArgs<R> s;
-    s.a = a.a; s.tw = a.tw; s.X = a.X; s.dim = a.dim; s.N = a.N; s.phase_fac = a.phase_fac;
+    s.a = a.a; s.tw = a.tw; s.tw_lo = a.tw_lo; s.X = a.X; s.dim = a.dim; s.N = a.N; s.phase_fac = a.phase_fac;
     s.scale = a.scale; s.pois_c = a.pois_c; s.pois_g0 = a.pois_g0; s.partial = a.partial;
     return s;
 }
@@ -220,14 +221,30 @@ static TmaGeom tma_geom(int X, int want_tx, int op, int E, const Tune& tu) {
     return g;
 }
 
+// Double-float twiddles: FP32 passes given a low-part table (the host passes
+// one for wave-function arrays only).  The drift and kinetic passes always act
+// on psi, the Poisson pass never does.
+template <typename R, int OP> constexpr bool df_only() { return sizeof(R) == 4 && (OP == OP_DRIFT || OP == OP_KIN); }
+template <typename R, int OP> constexpr bool df_never() { return sizeof(R) != 4 || OP == OP_POISSON; }
+template <typename R, int OP> static bool use_df(const typename Ops<R>::SP& a) {
+    if constexpr (df_never<R, OP>()) return false;
+    else if constexpr (df_only<R, OP>()) {
+        if (!a.tw_lo) throw std::logic_error("pass needs the low twiddle table");
+        return true;
+    } else {
+        return a.tw_lo != nullptr;
+    }
+}
+
 // Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
-template <int NN, typename R, int OP, int EPT>
+template <int NN, typename R, int OP, int EPT, bool DF>
 static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                          const Tune& tu, cudaStream_t st) {
     const TmaGeom g = tma_geom<NN, R>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP,
                                       tma_eff_e<NN, R, EPT>(), tu);
     TArgs<R> s;
     s.tw = a.tw;
+    s.tw_lo = a.tw_lo;
     s.X = a.X;
     s.N = NN;
     s.outer = outer;
@@ -247,7 +264,7 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.partial = a.partial;
     s.err = a.err;
     const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim);
-    auto kern = k_pencil_tma<NN, R, OP, EPT>;
+    auto kern = k_pencil_tma<NN, R, OP, EPT, DF>;
     const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
@@ -267,11 +284,22 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
 
 // tu.ept = 8 selects the register-lean variant (8 values per thread, two
 // blocks per SM) where it is valid; otherwise the default layout
+template <int NN, typename R, int OP, bool DF>
+static long launch_tma_df(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
+                          const Tune& tu, cudaStream_t st) {
+    if (tu.ept == 8) return launch_tma_e<NN, R, OP, 8, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    return launch_tma_e<NN, R, OP, 0, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+}
+
 template <int NN, typename R, int OP>
 static long launch_tma(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                        const Tune& tu, cudaStream_t st) {
-    if (tu.ept == 8) return launch_tma_e<NN, R, OP, 8>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
-    return launch_tma_e<NN, R, OP, 0>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    const bool df = use_df<R, OP>(a);
+    if constexpr (!df_never<R, OP>()) {
+        if (df) return launch_tma_df<NN, R, OP, true>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    }
+    if constexpr (!df_only<R, OP>()) return launch_tma_df<NN, R, OP, false>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    throw std::logic_error("launch_tma: unreachable twiddle mode");
 }
 
 template <typename R>
@@ -285,12 +313,14 @@ void Ops<R>::y_pass(int N, int outer, const SP& a, int sign, const Tune& tu, cud
         });
         return;
     }
+    const bool df = use_df<R, OP_FWD>(a);
     QX_FOR_N(N, {
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;
-        auto kern = sign < 0 ? k_y_pass<NN, R, -1> : k_y_pass<NN, R, +1>;
-        static int mt_cache[2] = {0, 0};
-        int& mt = mt_cache[sign < 0 ? 0 : 1];
+        auto kern = sign < 0 ? (df ? k_y_pass<NN, R, -1, true> : k_y_pass<NN, R, -1, false>)
+                             : (df ? k_y_pass<NN, R, +1, true> : k_y_pass<NN, R, +1, false>);
+        static int mt_cache[4] = {0, 0, 0, 0};
+        int& mt = mt_cache[(sign < 0 ? 0 : 1) + (df ? 2 : 0)];
         if (!mt) mt = max_threads(kern);
         const int tx = pick_tx(a.X, T, 1, tu.y_tx, sizeof(C), NN, mt);
         const int pitch = (tx * (int)sizeof(C) < 128) ? tx + 1 : tx;
@@ -302,23 +332,28 @@ void Ops<R>::y_pass(int N, int outer, const SP& a, int sign, const Tune& tu, cud
     });
 }
 
+// direct-load last-axis kernel of an op; the FP32 drift and kinetic passes
+// always take double-float twiddles, the Poisson pass never, the plain
+// transforms when `df` (a wave-function array)
 template <int NN, typename R>
-static void (*la_kernel(int op))(SArgs<R>) {
+static void (*la_kernel(int op, bool df))(SArgs<R>) {
+    constexpr bool f32 = sizeof(R) == 4;
     switch (op) {
-        case OP_FWD: return k_la_pass<NN, R, LA_FWD>;
-        case OP_INV: return k_la_pass<NN, R, LA_INV>;
-        case OP_DRIFT: return k_la_pass<NN, R, LA_DRIFT>;
-        case OP_POISSON: return k_la_pass<NN, R, LA_POISSON>;
-        case OP_KIN: return k_la_pass<NN, R, LA_KIN>;
+        case OP_FWD: return df ? k_la_pass<NN, R, LA_FWD, f32> : k_la_pass<NN, R, LA_FWD, false>;
+        case OP_INV: return df ? k_la_pass<NN, R, LA_INV, f32> : k_la_pass<NN, R, LA_INV, false>;
+        case OP_DRIFT: return k_la_pass<NN, R, LA_DRIFT, f32>;
+        case OP_POISSON: return k_la_pass<NN, R, LA_POISSON, false>;
+        case OP_KIN: return k_la_pass<NN, R, LA_KIN, f32>;
     }
     throw std::invalid_argument("la_pass: bad op");
 }
 
 template <int NN, typename R>
-static int la_max_threads(int op) {
-    static int cache[5] = {0, 0, 0, 0, 0};
-    if (!cache[op]) cache[op] = max_threads(la_kernel<NN, R>(op));
-    return cache[op];
+static int la_max_threads(int op, bool df) {
+    static int cache[10] = {0};
+    const int key = op + (df ? 5 : 0);
+    if (!cache[key]) cache[key] = max_threads(la_kernel<NN, R>(op, df));
+    return cache[key];
 }
 
 template <typename R>
@@ -329,7 +364,7 @@ long Ops<R>::la_blocks(int N, int X, int dim, int op, const Tune& tu) {
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;
         const int G = (dim == 3 && op == OP_POISSON) ? 2 : 1;
-        const int tx = pick_tx(X, T, G, tu.la_tx, sizeof(C), NN, la_max_threads<NN, R>(op));
+        const int tx = pick_tx(X, T, G, tu.la_tx, sizeof(C), NN, la_max_threads<NN, R>(op, X == NN));
         const long gy = dim == 3 ? (G == 2 ? NN / 2 : NN) : 1;
         return (long)(X / tx) * gy;
     });
@@ -341,7 +376,7 @@ static void launch_col0(const typename Ops<R>::SP& a, cudaStream_t st) {
     using C = cx_t<R>;
     constexpr int E0 = qx_lcm_radices(NN);
     dim3 blk(2, NN / E0, 1);
-    k_poisson_col0<NN, R><<<NN / 2, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.pois_c, a.pois_g0);
+    k_poisson_col0<NN, R><<<NN / 2, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.tw_lo, a.pois_c, a.pois_g0);
     QX_LAUNCH_CHECK();
 }
 
@@ -349,6 +384,7 @@ template <typename R>
 long Ops<R>::la_pass(int N, const SP& a, int op, const Tune& tu, cudaStream_t st) {
     using C = cx_t<R>;
     const SArgs<R> s = to_s<R>(a);
+    const bool df = sizeof(R) == 4 && a.tw_lo != nullptr;
     if (tu.tma) {
         QX_FOR_N(N, {
             const int d3 = a.dim == 3 ? 1 : 0;
@@ -372,12 +408,12 @@ long Ops<R>::la_pass(int N, const SP& a, int op, const Tune& tu, cudaStream_t st
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;
         const int G = (a.dim == 3 && op == OP_POISSON) ? 2 : 1;
-        const int tx = pick_tx(a.X, T, G, tu.la_tx, sizeof(C), NN, la_max_threads<NN, R>(op));
+        const int tx = pick_tx(a.X, T, G, tu.la_tx, sizeof(C), NN, la_max_threads<NN, R>(op, df));
         const int pitch = (tx * (int)sizeof(C) < 128) ? tx + 1 : tx;
         const size_t smem = (size_t)G * NN * pitch * sizeof(C);
         const unsigned gy = a.dim == 3 ? (G == 2 ? NN / 2 : NN) : 1;
         dim3 blk(tx, T, G), grd(a.X / tx, gy);
-        auto kern = la_kernel<NN, R>(op);
+        auto kern = la_kernel<NN, R>(op, df);
         set_smem(kern, smem);
         kern<<<grd, blk, smem, st>>>(s);
         QX_LAUNCH_CHECK();

@@ -108,12 +108,13 @@ __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(s
 // dynamic shared memory of a pass: NBUF tiles + twiddles + drift factors
 // (drift only) + column-0 stash (Poisson only) + 1 KB base-alignment slack
 template <typename R> __host__ __device__ constexpr size_t tma_smem_bytes(int N, int TX, int nbuf, int op) {
-    return (size_t)nbuf * align1k((size_t)N * TX * 2 * sizeof(R)) + (size_t)N * 2 * sizeof(R) +
+    return (size_t)nbuf * align1k((size_t)N * TX * 2 * sizeof(R)) + (size_t)N * 4 * sizeof(R) +
            (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) + 1024;
 }
 
 template <typename R> struct TArgs {
     const cx_t<R>* tw;   // exp(-2 pi i j/N), global
+    const cx_t<R>* tw_lo;  // exact - tw (FP32 double-float twiddles), global
     int X;               // columns (N for psi, N/2 for the packed half spectrum)
     int N;
     int outer;           // tiles along the non-pencil axis (z for y passes, y for z passes, 1 in 2D)
@@ -137,7 +138,7 @@ template <int N, typename R, int EPT> __host__ __device__ constexpr int tma_min_
     return (sizeof(R) == 4 && tma_eff_e<N, R, EPT>() <= 8) ? 2 : 1;
 }
 
-template <int N, typename R, int OP, int EPT>
+template <int N, typename R, int OP, int EPT, bool DF>
 __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
     k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
@@ -154,7 +155,8 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
     const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
     C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     C* tws = bufs + s.nbuf * tile_elems;
-    double2* bz = reinterpret_cast<double2*>(tws + N);
+    C* tws_lo = tws + N;
+    double2* bz = reinterpret_cast<double2*>(tws_lo + N);
     C* col0 = reinterpret_cast<C*>(bz + (OP == OP_DRIFT ? N : 0));
 
     auto coords = [&](long id, int j, int& c0, int& c1, int& c2) {
@@ -175,7 +177,10 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
     };
 
     // per-launch tables and barriers
-    for (int i = tid; i < N; i += nthr) tws[i] = s.tw[i];
+    for (int i = tid; i < N; i += nthr) {
+        tws[i] = s.tw[i];
+        if constexpr (DF) tws_lo[i] = s.tw_lo[i];
+    }
     if constexpr (OP == OP_DRIFT) {
         for (int i = tid; i < N; i += nthr) {
             const long n = signed_mode(i, N);
@@ -222,10 +227,15 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
         const int x = x0 + c;
         ColAcc<C> acc{tile + c, TX};
         C v[E];
+        if constexpr (OP == OP_INV) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
-        if constexpr (OP == OP_INV) fft_pencil<N, E, +1>(v, acc, t, tws);
-        else fft_pencil<N, E, -1>(v, acc, t, tws);
+            for (int e = 0; e < E; ++e) v[e] = acc(out_pos<N, E>(e, t));
+            ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
+        } else {
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+            fft_pencil<N, E, -1>(v, acc, t, tw_src<DF>(tws, tws_lo));
+        }
 
         bool store = true;
         if constexpr (OP == OP_KIN) {
@@ -247,8 +257,7 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
                 const double2 A = cis_d(s.phase_fac * (double)mxy);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const double2 w = dcmul(A, bz[out_pos<N, E>(e, t)]);
-                    v[e] = cmul(v[e], mk<C>((R)w.x, (R)w.y));
+                    v[e] = cmul_d(v[e], dcmul(A, bz[out_pos<N, E>(e, t)]));
                 }
             } else {
                 SArgs<R> sa;
@@ -285,28 +294,30 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
                     }
                 }
             }
-            // back to stage-0 order (a no-op when the plan's first and last
-            // radix agree) and inverse transform
-            if constexpr (!qx_out_is_in<N>()) {
-                __syncthreads();
+            // inverse transform: the forward stages undone in reverse order,
+            // from the forward output order back to the load order
+            ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
+            if (OP == OP_POISSON && s.col0_external && x0 == 0) {
+                // the stash was written in another order by other threads; a
+                // multi-stage inverse already synchronised the block
+                if constexpr (qx_nstages(N) == 1) __syncthreads();
+                if (c0ext) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
-                __syncthreads();
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
-            }
-            fft_pencil<N, E, +1>(v, acc, t, tws);
-            if (c0ext) {
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = col0[out_pos<N, E>(e, t)];
+                    for (int e = 0; e < E; ++e) v[e] = col0[in_pos<N, E, 0>(e, t)];
+                }
             }
         }
 
         if (store) {
             // finished tile -> buffer (natural order) -> tensor store
             __syncthreads();
+            if constexpr (OP == OP_FWD) {
 #pragma unroll
-            for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+                for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) acc(in_pos<N, E, 0>(e, t)) = v[e];
+            }
             fence_proxy_async();
             __syncthreads();
             if (tid == 0) {
@@ -342,11 +353,12 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
 // C'(k) = a C(k) + b conj C(-k) with a, b from the kx = 0 and kx = N/2
 // multipliers, then the inverse z transform.  blockDim = (2, N/E).
 template <int N, typename R>
-__global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, double pois_c, double pois_g0) {
+__global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, const cx_t<R>* tw_lo, double pois_c,
+                               double pois_g0) {
     using C = cx_t<R>;
     constexpr int E = qx_lcm_radices(N);
     constexpr int X = N / 2;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw);
     const int g = threadIdx.x, t = threadIdx.y;
     const int gi = blockIdx.x;
@@ -366,16 +378,16 @@ __global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, double pois_c, do
     C v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-        const int p = in_pos<N, E, 0>(e, t);
+        const int p = out_pos<N, E>(e, t);
         const long nz = signed_mode(p, N);
         const long mA = ny * ny + nz * nz, mB = mA + (long)X * X;
         const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
         const C cm = cconj(macc((N - p) % N));
         v[e] = cadd(cscale(acc(p), R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
     }
-    fft_pencil<N, E, +1>(v, acc, t, tw);
+    ifft_pencil_rev<N, E>(v, acc, t, tw_src<false>(tw, tw_lo));
 #pragma unroll
-    for (int e = 0; e < E; ++e) vh[base + (long)out_pos<N, E>(e, t) * pstride] = v[e];
+    for (int e = 0; e < E; ++e) vh[base + (long)in_pos<N, E, 0>(e, t) * pstride] = v[e];
 }
 
 }  // namespace qx
