@@ -109,6 +109,27 @@ template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, d
 
 __device__ __forceinline__ int signed_mode(int i, int N) { return i <= (N >> 1) ? i : i - N; }
 
+// elements 2q and 2q+1 of a complex row: one 16-byte access per lane in the
+// FP32 form (a lane-contiguous q then reads whole lines), two in FP64
+template <typename C> __device__ __forceinline__ void load_pair(const C* row, int q, C& a, C& b) {
+    if constexpr (sizeof(C) == 8) {
+        const float4 v = reinterpret_cast<const float4*>(row)[q];
+        a = mk<C>(v.x, v.y);
+        b = mk<C>(v.z, v.w);
+    } else {
+        a = row[2 * q];
+        b = row[2 * q + 1];
+    }
+}
+template <typename C> __device__ __forceinline__ void store_pair(C* row, int q, C a, C b) {
+    if constexpr (sizeof(C) == 8) {
+        reinterpret_cast<float4*>(row)[q] = make_float4(a.x, a.y, b.x, b.y);
+    } else {
+        row[2 * q] = a;
+        row[2 * q + 1] = b;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // deterministic block reductions (fixed tree, FP64)
 // ---------------------------------------------------------------------------
@@ -168,7 +189,7 @@ template <int N, typename R, int MODE>
 __global__ void __launch_bounds__(256, 3) k_x_fwd(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -224,7 +245,7 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -277,7 +298,7 @@ __global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -287,7 +308,8 @@ __global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
     for (int e = 0; e < EH; ++e) {
         const int q = in_pos<M, EH, 0>(e, t);
         if constexpr (SRC == XR_DENSITY) {
-            const C p0 = a.in[row * N + 2 * q], p1 = a.in[row * N + 2 * q + 1];
+            C p0, p1;
+            load_pair(a.in + row * N, q, p0, p1);
             z[e] = mk<C>(pr * (p0.x * p0.x + p0.y * p0.y - rm), pr * (p1.x * p1.x + p1.y * p1.y - rm));
         } else {
             const C pair = reinterpret_cast<const C*>(a.Vin + row * N)[q];
@@ -319,7 +341,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
     constexpr int T = qx_row_threads(N);
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
@@ -355,16 +377,15 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
         C ps[E];
 #pragma unroll
         for (int e = 0; e < EH; ++e) {
-            const int q = in_pos<M, EH, 0>(e, t);
-            ps[2 * e] = kick1<R>(a.in[row * N + 2 * q], z[e].x, a.dt);
-            ps[2 * e + 1] = kick1<R>(a.in[row * N + 2 * q + 1], z[e].y, a.dt);
+            C p0, p1;
+            load_pair(a.in + row * N, in_pos<M, EH, 0>(e, t), p0, p1);
+            ps[2 * e] = kick1<R>(p0, z[e].x, a.dt);
+            ps[2 * e + 1] = kick1<R>(p1, z[e].y, a.dt);
         }
         if constexpr (FLAGS & XC_WRITE_PSI) {
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
-                const int q = in_pos<M, EH, 0>(e, t);
-                a.out[row * N + 2 * q] = ps[2 * e];
-                a.out[row * N + 2 * q + 1] = ps[2 * e + 1];
+                store_pair(a.out + row * N, in_pos<M, EH, 0>(e, t), ps[2 * e], ps[2 * e + 1]);
             }
         }
         if constexpr (FLAGS & XC_FWD) {
@@ -420,7 +441,7 @@ template <int N, typename R, int SIGN, bool DF>
 __global__ void k_y_pass(SArgs<R> s) {
     using C = cx_t<R>;
     constexpr int E = qx_col_e(N);
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int TX = blockDim.x;
     const int c = threadIdx.x, t = threadIdx.y;
     const int pitch = col_pitch<C>(TX);
@@ -462,7 +483,7 @@ template <int N, typename R, int OP, bool DF>
 __global__ void k_la_pass(SArgs<R> s) {
     using C = cx_t<R>;
     constexpr int E = qx_col_e(N);
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int TX = blockDim.x, G = blockDim.z;
     const int c = threadIdx.x, t = threadIdx.y, g = threadIdx.z;
     const int pitch = col_pitch<C>(TX);

@@ -203,7 +203,7 @@ template <typename R>
 __global__ void k_spec_bin(const cx_t<R>* vh, int dim, int N, const int* __restrict__ tab, int nbins,
                            double* part_P, long long* part_c) {
     using C = cx_t<R>;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nw = blockDim.x >> 5, warp = threadIdx.x >> 5;
     double* hPall = reinterpret_cast<double*>(smem_raw);
     long long* hCall = reinterpret_cast<long long*>(hPall + nw * nbins);

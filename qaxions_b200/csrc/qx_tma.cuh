@@ -106,10 +106,11 @@ template <int N, typename R> __host__ __device__ constexpr int tma_e() {
 __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
 
 // dynamic shared memory of a pass: NBUF tiles + twiddles + drift factors
-// (drift only) + column-0 stash (Poisson only) + 1 KB base-alignment slack
+// (drift only) + column-0 stash (Poisson only) + 128-byte base-alignment slack (the
+// tensor-copy alignment of unswizzled tiles; tiles are 1 KB multiples)
 template <typename R> __host__ __device__ constexpr size_t tma_smem_bytes(int N, int TX, int nbuf, int op) {
     return (size_t)nbuf * align1k((size_t)N * TX * 2 * sizeof(R)) + (size_t)N * 4 * sizeof(R) +
-           (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) + 1024;
+           (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) + 128;
 }
 
 template <typename R> struct TArgs {
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
     k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
     constexpr int E = tma_eff_e<N, R, EPT>();
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[8];
     __shared__ int s_ok;
     __shared__ double red[32];
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
     const int nthr = TX * blockDim.y;
     const uint32_t tile_bytes = (uint32_t)((size_t)N * TX * sizeof(C));
     const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
-    C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     C* tws = bufs + s.nbuf * tile_elems;
     C* tws_lo = tws + N;
     double2* bz = reinterpret_cast<double2*>(tws_lo + N);
@@ -358,7 +359,7 @@ __global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, const cx_t<R>* tw
     using C = cx_t<R>;
     constexpr int E = qx_lcm_radices(N);
     constexpr int X = N / 2;
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     C* sm = reinterpret_cast<C*>(smem_raw);
     const int g = threadIdx.x, t = threadIdx.y;
     const int gi = blockIdx.x;
