@@ -134,9 +134,9 @@ int qx_time_steps(qx_field_t *h, int nsteps, int use_graph, float *ms);
 int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, double *ms, int *n_out);
 /* launch geometry overrides (0 = default): rows per x-pass block, tile columns
  * of y / last-axis passes, strided-pass kernel family (1 = TMA-fed persistent,
- * 0 = direct loads; -1 = keep), TMA ring depth, values per thread of the TMA
- * passes (8 = register-lean two-blocks-per-SM variant) */
-int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int ept);
+ * 0 = direct loads; -1 = keep), TMA ring depth, pencils per thread of the TMA
+ * passes (1 or 2; 0 = default: 2 in the FP32 form, FP64 always 1) */
+int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw);
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 int qx_sync(qx_field_t *h);
 

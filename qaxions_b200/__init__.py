@@ -341,11 +341,11 @@ class Field:
         raw = names.raw
         return [(raw[64 * i:64 * i + 64].split(b"\0")[0].decode(), float(ms[i])) for i in range(n.value)]
 
-    def set_tune(self, x_rows: int = 0, y_tx: int = 0, la_tx: int = 0, tma: int = -1, nbuf: int = 0, ept: int = 0):
+    def set_tune(self, x_rows: int = 0, y_tx: int = 0, la_tx: int = 0, tma: int = -1, nbuf: int = 0, pw: int = 0):
         """Launch geometry overrides (0 = default); tma 1/0 selects the TMA-fed
         persistent or the direct-load strided kernels (-1 keeps the current);
-        ept 8 selects the register-lean TMA pass variant."""
-        self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, ept)
+        pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
+        self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
 
     def device_pointers(self):
         p, v = _vp(), _vp()

@@ -263,12 +263,12 @@ int qx_profile_step(qx_field_t* h, int nsteps, int max_entries, char* names, dou
     });
 }
 
-int qx_set_tune(qx_field_t* h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int ept) {
+int qx_set_tune(qx_field_t* h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw) {
     return guarded(h, [&](qx::Field& f) {
         need(x_rows >= 0 && y_tx >= 0 && la_tx >= 0 && nbuf >= 0 && nbuf <= 8 && tma >= -1 && tma <= 1 &&
-                 (ept == 0 || ept == 8),
+                 pw >= 0 && pw <= 2,
              "tune values out of range");
-        f.tune().ept = ept;
+        f.tune().pw = pw;
         f.tune().x_rows = x_rows;
         f.tune().y_tx = y_tx;
         f.tune().la_tx = la_tx;

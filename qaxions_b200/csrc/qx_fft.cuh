@@ -46,6 +46,33 @@ template <int SIGN, typename C> __device__ __forceinline__ C cmul_si(C a) {
     return SIGN < 0 ? mk<C>(a.y, -a.x) : mk<C>(-a.y, a.x);
 }
 
+// Two pencils at the same position (adjacent columns of a strided tile),
+// transformed together: one 16-byte shared-memory access moves both values,
+// and every twiddle is loaded and indexed once for the two.  The codelets and
+// stage drivers below are written over a generic value type (C or CPair<C>).
+template <typename C> struct __align__(2 * sizeof(C)) CPair {
+    C a, b;
+};
+template <typename T> struct real_of { using type = decltype(T::x); };
+template <typename C> struct real_of<CPair<C>> { using type = decltype(C::x); };
+template <typename T> using real_t = typename real_of<T>::type;
+
+template <typename C> __device__ __forceinline__ CPair<C> cadd(CPair<C> u, CPair<C> v) {
+    return {cadd(u.a, v.a), cadd(u.b, v.b)};
+}
+template <typename C> __device__ __forceinline__ CPair<C> csub(CPair<C> u, CPair<C> v) {
+    return {csub(u.a, v.a), csub(u.b, v.b)};
+}
+template <typename C> __device__ __forceinline__ CPair<C> cscale(CPair<C> u, decltype(C::x) s) {
+    return {cscale(u.a, s), cscale(u.b, s)};
+}
+template <int SIGN, typename C> __device__ __forceinline__ CPair<C> cmul_si(CPair<C> u) {
+    return {cmul_si<SIGN>(u.a), cmul_si<SIGN>(u.b)};
+}
+// pencil h (0 or 1) of a value
+template <typename C> __device__ __forceinline__ C& pen(C& v, int) { return v; }
+template <typename C> __device__ __forceinline__ C& pen(CPair<C>& v, int h) { return h ? v.b : v.a; }
+
 // ---------------------------------------------------------------------------
 // Radix plans (compile time).  L = 2^e: [8]*(e/3) + [2^(e%3) if e%3] (e <= 3:
 // one stage of radix L) -- the radix-8 stages come first so that every
@@ -111,6 +138,9 @@ template <typename C> __device__ __forceinline__ C cscale_rsqrt2(C a) {
     return mk<C>(fma(a.x, Consts<R>::rsqrt2, a.x * Consts<R>::rsqrt2_lo),
                  fma(a.y, Consts<R>::rsqrt2, a.y * Consts<R>::rsqrt2_lo));
 }
+template <typename C> __device__ __forceinline__ CPair<C> cscale_rsqrt2(CPair<C> u) {
+    return {cscale_rsqrt2(u.a), cscale_rsqrt2(u.b)};
+}
 
 template <int SIGN, typename C> __device__ __forceinline__ void dft2(C* a) {
     C t = a[0];
@@ -128,10 +158,10 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft4(C* a) {
 }
 
 template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* a) {
-    using R = decltype(C::x);
+    using R = real_t<C>;
     const C s = cadd(a[1], a[2]);
     const C d = csub(a[1], a[2]);
-    const C m = mk<C>(a[0].x - R(0.5) * s.x, a[0].y - R(0.5) * s.y);
+    const C m = csub(a[0], cscale(s, R(0.5)));
     const C rot = cmul_si<SIGN>(cscale(d, Consts<R>::sqrt3_2));
     a[0] = cadd(a[0], s);
     a[1] = cadd(m, rot);
@@ -139,7 +169,6 @@ template <int SIGN, typename C> __device__ __forceinline__ void dft3(C* a) {
 }
 
 template <int SIGN, typename C> __device__ __forceinline__ void dft8(C* a) {
-    using R = decltype(C::x);
     C e[4] = {a[0], a[2], a[4], a[6]};
     C o[4] = {a[1], a[3], a[5], a[7]};
     dft4<SIGN>(e);
@@ -199,15 +228,32 @@ template <int SIGN, typename C> __device__ __forceinline__ C tw_mul(C v, const C
     if (SIGN > 0) w.y = -w.y;
     return cmul(v, w);
 }
+// v (w + l) with the small correction v l added before the final rounding
+template <typename C> __device__ __forceinline__ C df_mul(C v, C w, C l) {
+    const auto cx = v.x * l.x - v.y * l.y;
+    const auto cy = v.x * l.y + v.y * l.x;
+    return mk<C>(fma(v.x, w.x, fma(-v.y, w.y, cx)), fma(v.x, w.y, fma(v.y, w.x, cy)));
+}
 template <int SIGN, typename C> __device__ __forceinline__ C tw_mul(C v, const TwPair<C>& tw, int i) {
     C w = tw.hi[i], l = tw.lo[i];
     if (SIGN > 0) {
         w.y = -w.y;
         l.y = -l.y;
     }
-    const auto cx = v.x * l.x - v.y * l.y;
-    const auto cy = v.x * l.y + v.y * l.x;
-    return mk<C>(fma(v.x, w.x, fma(-v.y, w.y, cx)), fma(v.x, w.y, fma(v.y, w.x, cy)));
+    return df_mul(v, w, l);
+}
+template <int SIGN, typename C> __device__ __forceinline__ CPair<C> tw_mul(CPair<C> v, const C* tw, int i) {
+    C w = tw[i];
+    if (SIGN > 0) w.y = -w.y;
+    return {cmul(v.a, w), cmul(v.b, w)};
+}
+template <int SIGN, typename C> __device__ __forceinline__ CPair<C> tw_mul(CPair<C> v, const TwPair<C>& tw, int i) {
+    C w = tw.hi[i], l = tw.lo[i];
+    if (SIGN > 0) {
+        w.y = -w.y;
+        l.y = -l.y;
+    }
+    return {df_mul(v.a, w, l), df_mul(v.b, w, l)};
 }
 
 template <int L, int E, int SIGN, int s, typename C, typename Acc, typename TW>

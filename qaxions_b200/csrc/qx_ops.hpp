@@ -20,7 +20,7 @@ struct Tune {
     int la_tx = 0;    // columns per tile in last-axis passes
     int tma = 1;      // strided passes: 1 = persistent TMA-fed kernels, 0 = direct-load kernels
     int nbuf = 0;     // TMA ring depth (0 = as many 64 KB-class tiles as fit in ~200 KB)
-    int ept = 0;      // values per thread of TMA passes (0 = default, 8 = register-lean variant)
+    int pw = 0;       // pencils per thread of TMA passes (0 = default: 2 in FP32, 1 in FP64)
 };
 
 template <typename R> struct Ops {

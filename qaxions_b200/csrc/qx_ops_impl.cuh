@@ -198,16 +198,16 @@ struct TmaGeom {
     size_t tile_bytes;
 };
 
-template <int NN, typename R>
-static TmaGeom tma_geom(int X, int want_tx, int op, int E, const Tune& tu) {
+template <int NN, typename R, int PW>
+static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
     using C = cx_t<R>;
     TmaGeom g;
-    g.T = NN / E;
+    g.T = NN / tma_e<NN, R, PW>();
     // default tile: 8 columns (64-byte rows for c64, 128-byte rows for c128) and
     // a 3-deep ring, which lets two FP32 blocks share an SM (measured best at
     // 512^3 against 16 columns / deeper rings)
     int tx = want_tx > 0 ? want_tx : 8;
-    while (tx > 1 && ((X % tx) || tx * g.T > 512)) tx >>= 1;
+    while (tx > PW && ((X % tx) || (tx / PW) * g.T > tma_max_threads<PW>())) tx >>= 1;
     g.TX = tx;
     g.box = NN <= 256 ? NN : 256;
     g.nbox = NN / g.box;
@@ -237,11 +237,10 @@ template <typename R, int OP> static bool use_df(const typename Ops<R>::SP& a) {
 }
 
 // Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
-template <int NN, typename R, int OP, int EPT, bool DF>
+template <int NN, typename R, int OP, int PW, bool DF>
 static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                          const Tune& tu, cudaStream_t st) {
-    const TmaGeom g = tma_geom<NN, R>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP,
-                                      tma_eff_e<NN, R, EPT>(), tu);
+    const TmaGeom g = tma_geom<NN, R, PW>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
     TArgs<R> s;
     s.tw = a.tw;
     s.tw_lo = a.tw_lo;
@@ -264,31 +263,32 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.partial = a.partial;
     s.err = a.err;
     const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim);
-    auto kern = k_pencil_tma<NN, R, OP, EPT, DF>;
+    auto kern = k_pencil_tma<NN, R, OP, PW, DF>;
     const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
     const int key = g.nbuf * 8 + (g.TX == 16 ? 4 : g.TX == 8 ? 3 : g.TX == 4 ? 2 : g.TX == 2 ? 1 : 0);
     int& bps = bps_cache[key & 63];
     if (!bps) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, g.TX * g.T, smem) != cudaSuccess || bps < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, (g.TX / PW) * g.T, smem) != cudaSuccess || bps < 1)
             bps = 1;
     }
     long grid = (long)sm_count() * bps;
     if (grid > s.n_tiles) grid = s.n_tiles;
-    dim3 blk(g.TX, g.T, 1);
+    dim3 blk(g.TX / PW, g.T, 1);
     kern<<<(unsigned)grid, blk, smem, st>>>(tm, s);
     QX_LAUNCH_CHECK();
     return grid;
 }
 
-// tu.ept = 8 selects the register-lean variant (8 values per thread, two
-// blocks per SM) where it is valid; otherwise the default layout
+// pencils per thread: tu.pw, default 2 in the FP32 form (paired columns), 1 in FP64
 template <int NN, typename R, int OP, bool DF>
 static long launch_tma_df(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                           const Tune& tu, cudaStream_t st) {
-    if (tu.ept == 8) return launch_tma_e<NN, R, OP, 8, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
-    return launch_tma_e<NN, R, OP, 0, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    if constexpr (sizeof(R) == 4) {
+        if (tu.pw != 1) return launch_tma_e<NN, R, OP, 2, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    }
+    return launch_tma_e<NN, R, OP, 1, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
 }
 
 template <int NN, typename R, int OP>

@@ -24,6 +24,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
 
 #include "qx_kernels.cuh"
 #include "qx_ops.hpp"
@@ -98,10 +99,19 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // persistent TMA pencil pass
 // ---------------------------------------------------------------------------
 
-// elements per thread of a strided pass
-template <int N, typename R> __host__ __device__ constexpr int tma_e() {
-    return (N >= 256 && sizeof(R) == 4) ? 16 : qx_lcm_radices(N);
+// Pencils per thread of a strided pass: PW = 2 (FP32 only) gives every thread
+// two adjacent columns, transformed together as CPair values, so each shared-
+// memory access moves 16 bytes and each twiddle is loaded once for both.
+template <int PW, typename C> using pencil_val_t = typename std::conditional<PW == 2, CPair<C>, C>::type;
+
+// elements per thread (per pencil) of a strided pass
+template <int N, typename R, int PW> __host__ __device__ constexpr int tma_e() {
+    return PW == 2 ? qx_lcm_radices(N) : ((N >= 256 && sizeof(R) == 4) ? 16 : qx_lcm_radices(N));
 }
+// launch bounds: one-pencil blocks take up to 512 threads (one per SM), paired
+// blocks up to 256 threads with two blocks per SM
+template <int PW> __host__ __device__ constexpr int tma_max_threads() { return PW == 2 ? 256 : 512; }
+template <int PW> __host__ __device__ constexpr int tma_min_blocks() { return PW == 2 ? 2 : 1; }
 
 __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
 
@@ -129,29 +139,23 @@ template <typename R> struct TArgs {
     int* err;            // set to 1 when a wait timed out
 };
 
-// elements per thread actually used: EPT when it is a valid choice for N
-// (a multiple of every radix, at most N), else the default
-template <int N, typename R, int EPT> __host__ __device__ constexpr int tma_eff_e() {
-    return (EPT > 0 && EPT % qx_lcm_radices(N) == 0 && EPT <= N) ? EPT : tma_e<N, R>();
-}
-// FP32 tiles with <= 8 values per thread fit two 512-thread blocks per SM
-template <int N, typename R, int EPT> __host__ __device__ constexpr int tma_min_blocks() {
-    return (sizeof(R) == 4 && tma_eff_e<N, R, EPT>() <= 8) ? 2 : 1;
-}
-
-template <int N, typename R, int OP, int EPT, bool DF>
-__global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
+// blockDim = (TX / PW, N / E): thread (c, t) owns columns x0 + PW c + h (h < PW)
+template <int N, typename R, int OP, int PW, bool DF>
+__global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
     k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
-    constexpr int E = tma_eff_e<N, R, EPT>();
+    using P = pencil_val_t<PW, C>;
+    static_assert(PW == 1 || sizeof(R) == 4, "paired pencils are an FP32 layout");
+    constexpr int E = tma_e<N, R, PW>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[8];
     __shared__ int s_ok;
     __shared__ double red[32];
     const int TX = s.TX;
+    const int TG = TX / PW;  // pencil groups per tile row
     const int c = threadIdx.x, t = threadIdx.y;
-    const int tid = c + TX * t;
-    const int nthr = TX * blockDim.y;
+    const int tid = c + TG * t;
+    const int nthr = TG * blockDim.y;
     const uint32_t tile_bytes = (uint32_t)((size_t)N * TX * sizeof(C));
     const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
     C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
@@ -225,9 +229,9 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
         C* tile = bufs + b * tile_elems;
         const int x0 = (int)(id % s.tiles_x) * TX;
         const int o = (int)(id / s.tiles_x);
-        const int x = x0 + c;
-        ColAcc<C> acc{tile + c, TX};
-        C v[E];
+        const int xb = x0 + PW * c;  // column of pencil 0 of this thread
+        ColAcc<P> acc{reinterpret_cast<P*>(tile) + c, TG};
+        P v[E];
         if constexpr (OP == OP_INV) {
 #pragma unroll
             for (int e = 0; e < E; ++e) v[e] = acc(out_pos<N, E>(e, t));
@@ -238,27 +242,39 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
             fft_pencil<N, E, -1>(v, acc, t, tw_src<DF>(tws, tws_lo));
         }
 
-        bool store = true;
-        if constexpr (OP == OP_KIN) {
+        // |n|^2 contribution of x (and y in 3D) of pencil h
+        auto mxy_of = [&](int h) {
+            const int x = xb + h;
             const int nx = (s.X == N) ? signed_mode(x, N) : x;
             const int ny = s.la3d ? signed_mode(o, N) : 0;
-            const long mxy = (long)nx * nx + (long)ny * ny;
+            return (long)nx * nx + (long)ny * ny;
+        };
+        bool store = true;
+        if constexpr (OP == OP_KIN) {
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const int nz = signed_mode(out_pos<N, E>(e, t), N);
-                kin += (double)(mxy + (long)nz * nz) * ((double)v[e].x * (double)v[e].x + (double)v[e].y * (double)v[e].y);
+            for (int h = 0; h < PW; ++h) {
+                const long mxy = mxy_of(h);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int nz = signed_mode(out_pos<N, E>(e, t), N);
+                    const C u = pen(v[e], h);
+                    kin += (double)(mxy + (long)nz * nz) * ((double)u.x * (double)u.x + (double)u.y * (double)u.y);
+                }
             }
             store = false;
         } else if constexpr (OP == OP_DRIFT || OP == OP_POISSON) {
-            const int nx = (s.X == N) ? signed_mode(x, N) : x;
-            const int ny = s.la3d ? signed_mode(o, N) : 0;
-            const long mxy = (long)nx * nx + (long)ny * ny;
-            const bool c0ext = (OP == OP_POISSON) && s.col0_external && x0 == 0 && c == 0;
+            // column 0 of the tile row (pencil 0 of thread group 0)
+            const bool has_col0 = x0 == 0 && c == 0;
+            const bool c0ext = (OP == OP_POISSON) && s.col0_external && has_col0;
             if constexpr (OP == OP_DRIFT) {
-                const double2 A = cis_d(s.phase_fac * (double)mxy);
+                double2 A[PW];
+#pragma unroll
+                for (int h = 0; h < PW; ++h) A[h] = cis_d(s.phase_fac * (double)mxy_of(h));
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    v[e] = cmul_d(v[e], dcmul(A, bz[out_pos<N, E>(e, t)]));
+                    const double2 bze = bz[out_pos<N, E>(e, t)];
+#pragma unroll
+                    for (int h = 0; h < PW; ++h) pen(v[e], h) = cmul_d(pen(v[e], h), dcmul(A[h], bze));
                 }
             } else {
                 SArgs<R> sa;
@@ -268,7 +284,7 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
                     // 3D: column 0 (kx = 0 and N/2 packed) is paired with its mirror
                     // row by k_poisson_col0; keep the forward result for it
 #pragma unroll
-                    for (int e = 0; e < E; ++e) col0[out_pos<N, E>(e, t)] = v[e];
+                    for (int e = 0; e < E; ++e) col0[out_pos<N, E>(e, t)] = pen(v[e], 0);
                 } else if (x0 == 0 && !s.col0_external) {
                     // 2D: the mirror -k_y of column 0 lies in the same pencil
                     __syncthreads();
@@ -282,16 +298,19 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
                             const long np = signed_mode(p, N);
                             const long mA = np * np, mB = mA + (long)(N / 2) * (N / 2);
                             const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
-                            const C cm = cconj(acc((N - p) % N));
-                            v[e] = cadd(cscale(v[e], R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
+                            const C cm = cconj(pen(acc((N - p) % N), 0));
+                            pen(v[e], 0) = cadd(cscale(pen(v[e], 0), R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
                         }
                     }
                 }
-                if (!(x0 == 0 && c == 0)) {
+#pragma unroll
+                for (int h = 0; h < PW; ++h) {
+                    if (h == 0 && has_col0) continue;
+                    const long mxy = mxy_of(h);
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
                         const int nz = signed_mode(out_pos<N, E>(e, t), N);
-                        v[e] = cscale(v[e], pois_mult<R>(mxy + (long)nz * nz, sa));
+                        pen(v[e], h) = cscale(pen(v[e], h), pois_mult<R>(mxy + (long)nz * nz, sa));
                     }
                 }
             }
@@ -304,7 +323,7 @@ __global__ void __launch_bounds__(512, (tma_min_blocks<N, R, EPT>()))
                 if constexpr (qx_nstages(N) == 1) __syncthreads();
                 if (c0ext) {
 #pragma unroll
-                    for (int e = 0; e < E; ++e) v[e] = col0[in_pos<N, E, 0>(e, t)];
+                    for (int e = 0; e < E; ++e) pen(v[e], 0) = col0[in_pos<N, E, 0>(e, t)];
                 }
             }
         }
