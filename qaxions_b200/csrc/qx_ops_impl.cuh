@@ -208,6 +208,10 @@ static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
     // 512^3 against 16 columns / deeper rings)
     int tx = want_tx > 0 ? want_tx : 8;
     while (tx > PW && ((X % tx) || (tx / PW) * g.T > tma_max_threads<PW>())) tx >>= 1;
+    if (tma_tx_fixed<NN>() > 0) {  // compiled-in tile width
+        tx = tma_tx_fixed<NN>();
+        if ((X % tx) || (tx / PW) * g.T > tma_max_threads<PW>()) throw std::logic_error("TMA tile width does not fit");
+    }
     g.TX = tx;
     g.box = NN <= 256 ? NN : 256;
     g.nbox = NN / g.box;

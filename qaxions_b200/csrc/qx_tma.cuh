@@ -112,6 +112,9 @@ template <int N, typename R, int PW> __host__ __device__ constexpr int tma_e() {
 // blocks up to 256 threads with two blocks per SM
 template <int PW> __host__ __device__ constexpr int tma_max_threads() { return PW == 2 ? 256 : 512; }
 template <int PW> __host__ __device__ constexpr int tma_min_blocks() { return PW == 2 ? 2 : 1; }
+// tile columns: 8 (64-byte FP32 / 128-byte FP64 rows), fixed at compile time so
+// shared-memory addresses fold to constants; smaller grids pick at run time
+template <int N> __host__ __device__ constexpr int tma_tx_fixed() { return N >= 16 ? 8 : 0; }
 
 __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
 
@@ -149,9 +152,9 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
     constexpr int E = tma_e<N, R, PW>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[8];
-    __shared__ int s_ok;
+    __shared__ int s_abort;
     __shared__ double red[32];
-    const int TX = s.TX;
+    const int TX = tma_tx_fixed<N>() > 0 ? tma_tx_fixed<N>() : s.TX;
     const int TG = TX / PW;  // pencil groups per tile row
     const int c = threadIdx.x, t = threadIdx.y;
     const int tid = c + TG * t;
@@ -194,6 +197,7 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
         }
     }
     if (tid == 0) {
+        s_abort = 0;
         for (int b = 0; b < s.nbuf; ++b) mbar_init(smem_u32(&mbar[b]), 1);
         fence_mbar_init();
         for (int k = 0; k < s.nbuf - 1; ++k) {
@@ -204,28 +208,16 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
     __syncthreads();
 
     double kin = 0.0;
-    for (int k = 0;; ++k) {
+    int k = 0;
+    for (;; ++k) {
         const long id = blockIdx.x + (long)k * gridDim.x;
         if (id >= s.n_tiles) break;
         const int b = k % s.nbuf;
         const uint32_t parity = (uint32_t)((k / s.nbuf) & 1);
-        if (tid == 0) s_ok = mbar_wait_bounded(smem_u32(&mbar[b]), parity) ? 1 : 0;
-        __syncthreads();
-        if (!s_ok) {
-            if (tid == 0) {
-                atomicExch(s.err, 1);
-                for (int j = 1; j < s.nbuf - 1; ++j) {  // this block's other loads in flight
-                    const long jd = id + (long)j * gridDim.x;
-                    if (jd < s.n_tiles)
-                        mbar_wait_bounded(smem_u32(&mbar[(k + j) % s.nbuf]), (uint32_t)(((k + j) / s.nbuf) & 1),
-                                          1LL << 28);
-                }
-                bulk_wait_all();
-            }
-            __syncthreads();
-            return;
-        }
-        (void)mbar_try(smem_u32(&mbar[b]), parity);  // acquire the TMA writes in every thread
+        // every thread waits for (and acquires) the tile itself; a time-out is
+        // recorded and acted on at the tile's last barrier, where all threads
+        // read the same flag
+        if (!mbar_wait_bounded(smem_u32(&mbar[b]), parity)) s_abort = 1;
         C* tile = bufs + b * tile_elems;
         const int x0 = (int)(id % s.tiles_x) * TX;
         const int o = (int)(id / s.tiles_x);
@@ -340,6 +332,7 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
             }
             fence_proxy_async();
             __syncthreads();
+            if (s_abort) break;
             if (tid == 0) {
                 for (int j = 0; j < s.nbox; ++j) {
                     int c0, c1, c2;
@@ -350,6 +343,7 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
             }
         } else {
             __syncthreads();
+            if (s_abort) break;
         }
         // refill the buffer of tile k-1 (its store has been read out) with tile k+NBUF-1
         if (tid == 0) {
@@ -360,6 +354,21 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
                 issue_load(nid, (k + s.nbuf - 1) % s.nbuf);
             }
         }
+    }
+    if (s_abort) {
+        // a tile did not arrive in time: flag it, wait (bounded) for this
+        // block's loads still in flight and for its stores, and leave
+        if (tid == 0) {
+            atomicExch(s.err, 1);
+            for (int j = 0; j < s.nbuf - 1; ++j) {  // tiles k .. k+NBUF-2 were requested
+                const long jd = blockIdx.x + (long)(k + j) * gridDim.x;
+                if (jd < s.n_tiles)
+                    mbar_wait_bounded(smem_u32(&mbar[(k + j) % s.nbuf]), (uint32_t)(((k + j) / s.nbuf) & 1),
+                                      1LL << 28);
+            }
+            bulk_wait_all();
+        }
+        return;
     }
     if (tid == 0) bulk_wait_all();
     if constexpr (OP == OP_KIN) {
