@@ -199,11 +199,25 @@ template <int r, int SIGN, typename C> __device__ __forceinline__ void dft(C* a)
 // a `sync()` that is a barrier over every thread sharing the buffer.
 // ---------------------------------------------------------------------------
 
-// position held in v[e] before stage s (stage-s input order)
-template <int L, int E, int s> __device__ __forceinline__ int in_pos(int e, int t) {
-    constexpr int r = qx_radix(L, s);
+// Butterfly column j of block b of thread t at stage s.  J0 = 1 pairs the
+// stage-0 columns, j = 2t + 2T (b/2) + (b%2), so that a thread holds the
+// adjacent positions 2q and 2q+1 of its inputs: the layout in which an r2c
+// transform of length L/2 leaves its real output and a c2r transform takes
+// its real input, so a row pass can chain them without a shared-memory copy.
+template <int L, int E, int s, int J0> __device__ __forceinline__ int stage_j(int b, int t) {
     constexpr int T = L / E;
-    return t + (e / r) * T + (e % r) * (L / r);
+    if constexpr (s == 0 && J0 == 1) {
+        static_assert((E / qx_radix(L, 0)) % 2 == 0, "paired stage-0 columns need an even number of blocks");
+        return 2 * t + 2 * T * (b >> 1) + (b & 1);
+    } else {
+        return t + b * T;
+    }
+}
+
+// position held in v[e] before stage s (stage-s input order)
+template <int L, int E, int s, int J0 = 0> __device__ __forceinline__ int in_pos(int e, int t) {
+    constexpr int r = qx_radix(L, s);
+    return stage_j<L, E, s, J0>(e / r, t) + (e % r) * (L / r);
 }
 // position held in v[e] after the last stage (natural-order output)
 template <int L, int E> __device__ __forceinline__ int out_pos(int e, int t) {
@@ -256,18 +270,17 @@ template <int SIGN, typename C> __device__ __forceinline__ CPair<C> tw_mul(CPair
     return {df_mul(v.a, w, l), df_mul(v.b, w, l)};
 }
 
-template <int L, int E, int SIGN, int s, typename C, typename Acc, typename TW>
+template <int L, int E, int SIGN, int s, int J0, typename C, typename Acc, typename TW>
 __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const TW& tw) {
     constexpr int S = qx_nstages(L);
     if constexpr (s < S) {
         constexpr int r = qx_radix(L, s);
         constexpr int Ns = qx_span(L, s);
-        constexpr int T = L / E;
         static_assert(E % r == 0, "radix must divide elements per thread");
         constexpr int nb = E / r;
 #pragma unroll
         for (int b = 0; b < nb; ++b) {
-            const int j = t + b * T;
+            const int j = stage_j<L, E, s, J0>(b, t);
             if constexpr (Ns > 1) {
                 const int k = j % Ns;
                 constexpr int stw = L / (Ns * r);
@@ -281,7 +294,7 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const TW&
             acc.sync();
 #pragma unroll
             for (int b = 0; b < nb; ++b) {
-                const int j = t + b * T;
+                const int j = stage_j<L, E, s, J0>(b, t);
                 const int idxD = (j / Ns) * Ns * r + (j % Ns);
 #pragma unroll
                 for (int m = 0; m < r; ++m) acc(idxD + m * Ns) = v[b * r + m];
@@ -289,16 +302,16 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const TW&
             acc.sync();
 #pragma unroll
             for (int e = 0; e < E; ++e) v[e] = acc(in_pos<L, E, s + 1>(e, t));
-            fft_stages<L, E, SIGN, s + 1>(v, acc, t, tw);
+            fft_stages<L, E, SIGN, s + 1, J0>(v, acc, t, tw);
         }
     }
 }
 
-// Full transform: v in stage-0 input order on entry (see in_pos<L,E,0>),
+// Full transform: v in stage-0 input order on entry (see in_pos<L,E,0,J0>),
 // natural-order outputs at out_pos<L,E> on exit.
-template <int L, int E, int SIGN, typename C, typename Acc, typename TW>
+template <int L, int E, int SIGN, int J0 = 0, typename C, typename Acc, typename TW>
 __device__ __forceinline__ void fft_pencil(C (&v)[E], Acc& acc, int t, const TW& tw) {
-    fft_stages<L, E, SIGN, 0>(v, acc, t, tw);
+    fft_stages<L, E, SIGN, 0, J0>(v, acc, t, tw);
 }
 
 // Twiddle source of a transform: DF = true selects double-float twiddles in
@@ -322,28 +335,26 @@ __device__ __forceinline__ auto tw_src(const C* hi, const C* lo) {
 
 // Position held by v[e] in the OUTPUT order of forward stage s (where stage s
 // writes its results); for the last stage this is out_pos.
-template <int L, int E, int s> __device__ __forceinline__ int stage_out_pos(int e, int t) {
+template <int L, int E, int s, int J0 = 0> __device__ __forceinline__ int stage_out_pos(int e, int t) {
     constexpr int r = qx_radix(L, s);
     constexpr int Ns = qx_span(L, s);
-    constexpr int T = L / E;
-    const int j = t + (e / r) * T;
+    const int j = stage_j<L, E, s, J0>(e / r, t);
     return (j / Ns) * Ns * r + (j % Ns) + (e % r) * Ns;
 }
 
 // Undo forward stage s (inverse butterfly, then conjugate twiddles), then
 // move on to stage s-1.  Entry: v in stage_out_pos<s> order; exit of the
-// whole chain: v in stage-0 input order (in_pos<L,E,0>).
-template <int L, int E, int s, typename C, typename Acc, typename TW>
+// whole chain: v in stage-0 input order (in_pos<L,E,0,J0>).
+template <int L, int E, int s, int J0, typename C, typename Acc, typename TW>
 __device__ __forceinline__ void ifft_rev_stages(C (&v)[E], Acc& acc, int t, const TW& tw) {
     constexpr int r = qx_radix(L, s);
     constexpr int Ns = qx_span(L, s);
-    constexpr int T = L / E;
     constexpr int nb = E / r;
 #pragma unroll
     for (int b = 0; b < nb; ++b) {
         dft<r, +1>(&v[b * r]);
         if constexpr (Ns > 1) {
-            const int k = (t + b * T) % Ns;
+            const int k = stage_j<L, E, s, J0>(b, t) % Ns;
             constexpr int stw = L / (Ns * r);
 #pragma unroll
             for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<+1>(v[b * r + m], tw, k * m * stw);
@@ -355,17 +366,17 @@ __device__ __forceinline__ void ifft_rev_stages(C (&v)[E], Acc& acc, int t, cons
         for (int e = 0; e < E; ++e) acc(in_pos<L, E, s>(e, t)) = v[e];
         acc.sync();
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = acc(stage_out_pos<L, E, s - 1>(e, t));
-        ifft_rev_stages<L, E, s - 1>(v, acc, t, tw);
+        for (int e = 0; e < E; ++e) v[e] = acc(stage_out_pos<L, E, s - 1, J0>(e, t));
+        ifft_rev_stages<L, E, s - 1, J0>(v, acc, t, tw);
     }
 }
 
 // Unnormalised inverse transform (x L) that exactly undoes fft_pencil<L,E,-1>:
 // v in natural output order (out_pos<L,E>) on entry, in stage-0 input order
-// (in_pos<L,E,0>, lane-contiguous natural order) on exit.
-template <int L, int E, typename C, typename Acc, typename TW>
+// (in_pos<L,E,0,J0>) on exit.
+template <int L, int E, int J0 = 0, typename C, typename Acc, typename TW>
 __device__ __forceinline__ void ifft_pencil_rev(C (&v)[E], Acc& acc, int t, const TW& tw) {
-    ifft_rev_stages<L, E, qx_nstages(L) - 1>(v, acc, t, tw);
+    ifft_rev_stages<L, E, qx_nstages(L) - 1, J0>(v, acc, t, tw);
 }
 
 }  // namespace qx

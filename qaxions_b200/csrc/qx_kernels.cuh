@@ -53,6 +53,20 @@ __device__ __forceinline__ unsigned warp_lanes_mask() {
 }
 __host__ __device__ constexpr int row_smem_elems(int n) { return n + (n >> 4) + 1; }
 
+// Row passes chain an N-point c2c transform with the N/2-point core of an
+// r2c/c2r transform.  When both plans start with the same radix, the N-point
+// transform runs with paired stage-0 columns (stage_j, J0 = 1): thread t then
+// holds positions 2q and 2q+1 for every q = in_pos<N/2, E/2, 0>(e, t), the
+// pairs the half-length transform consumes or produces, in registers
+// v[row_pair_idx<N>(e, h)] (h = 0, 1).
+template <int N> __host__ __device__ constexpr bool row_paired() {
+    return N >= 16 && qx_radix(N, 0) == qx_radix(N / 2, 0) && (qx_row_efull(N) / qx_radix(N, 0)) % 2 == 0;
+}
+template <int N> __host__ __device__ constexpr int row_pair_idx(int e, int h) {
+    constexpr int r0 = qx_radix(N, 0);
+    return row_paired<N>() ? (2 * (e / r0) + h) * r0 + e % r0 : 2 * e + h;
+}
+
 // column of a strided tile: element p of this pencil at base[p * pitch]
 template <typename C> struct ColAcc {
     C* base;
@@ -249,35 +263,41 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
     C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
     const int t = threadIdx.x;
     const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
+    constexpr bool PAIRED = row_paired<N>();
     const C* src = a.in + row * N;
     C v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = src[out_pos<N, E>(e, t)];
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    ifft_pencil_rev<N, E>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
+    ifft_pencil_rev<N, E, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
     const R sc = (R)a.scale;
     C* dst = a.out + row * N;
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-        v[e] = cscale(v[e], sc);
-        dst[in_pos<N, E, 0>(e, t)] = v[e];
+    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], sc);
+    if constexpr (PAIRED) {
+#pragma unroll
+        for (int e = 0; e < EH; ++e)
+            store_pair(dst, in_pos<M, EH, 0>(e, t), v[row_pair_idx<N>(e, 0)], v[row_pair_idx<N>(e, 1)]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) dst[in_pos<N, E, 0>(e, t)] = v[e];
     }
     if constexpr (MODE == XI_R2C) {
-        // stage the real source in smem (as R[N] over the same buffer)
-        R* rs = reinterpret_cast<R*>(sm);
-        acc.sync();
         const R pr = (R)a.pref, rm = (R)a.rho_mean;
+        auto src_of = [&](const C& u) { return pr * (u.x * u.x + u.y * u.y - rm); };
+        C z[EH];  // (rho[2q], rho[2q+1]), q = in_pos<M, EH, 0>(e, t)
+        if constexpr (PAIRED) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int p = in_pos<N, E, 0>(e, t);
-            const R rho = v[e].x * v[e].x + v[e].y * v[e].y;
-            rs[p] = pr * (rho - rm);
-        }
-        acc.sync();
-        C z[EH];
+            for (int e = 0; e < EH; ++e) z[e] = mk<C>(src_of(v[row_pair_idx<N>(e, 0)]), src_of(v[row_pair_idx<N>(e, 1)]));
+        } else {
+            // stage the real source in smem (as R[N] over the same buffer)
+            R* rs = reinterpret_cast<R*>(sm);
+            acc.sync();
 #pragma unroll
-        for (int e = 0; e < EH; ++e) {
-            z[e] = reinterpret_cast<const C*>(rs)[in_pos<M, EH, 0>(e, t)];  // (rho[2q], rho[2q+1])
+            for (int e = 0; e < E; ++e) rs[in_pos<N, E, 0>(e, t)] = src_of(v[e]);
+            acc.sync();
+#pragma unroll
+            for (int e = 0; e < EH; ++e) z[e] = reinterpret_cast<const C*>(rs)[in_pos<M, EH, 0>(e, t)];
         }
         fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
         acc.sync();
@@ -374,33 +394,40 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
         for (int e = 0; e < EH; ++e) vrow[in_pos<M, EH, 0>(e, t)] = z[e];
     }
     if constexpr (FLAGS & XC_KICK) {
-        C ps[E];
+        constexpr bool PAIRED = row_paired<N>();
+        C ps[E];  // kicked psi: position 2q+h in ps[row_pair_idx<N>(e, h)]
 #pragma unroll
         for (int e = 0; e < EH; ++e) {
             C p0, p1;
             load_pair(a.in + row * N, in_pos<M, EH, 0>(e, t), p0, p1);
-            ps[2 * e] = kick1<R>(p0, z[e].x, a.dt);
-            ps[2 * e + 1] = kick1<R>(p1, z[e].y, a.dt);
+            ps[row_pair_idx<N>(e, 0)] = kick1<R>(p0, z[e].x, a.dt);
+            ps[row_pair_idx<N>(e, 1)] = kick1<R>(p1, z[e].y, a.dt);
         }
         if constexpr (FLAGS & XC_WRITE_PSI) {
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
-                store_pair(a.out + row * N, in_pos<M, EH, 0>(e, t), ps[2 * e], ps[2 * e + 1]);
+                store_pair(a.out + row * N, in_pos<M, EH, 0>(e, t), ps[row_pair_idx<N>(e, 0)], ps[row_pair_idx<N>(e, 1)]);
             }
         }
         if constexpr (FLAGS & XC_FWD) {
-            acc.sync();
-#pragma unroll
-            for (int e = 0; e < EH; ++e) {
-                const int q = in_pos<M, EH, 0>(e, t);
-                acc(2 * q) = ps[2 * e];
-                acc(2 * q + 1) = ps[2 * e + 1];
-            }
-            acc.sync();
             C v[E];
+            if constexpr (PAIRED) {
+                // already in the paired stage-0 input order
 #pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
-            fft_pencil<N, E, -1>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
+                for (int e = 0; e < E; ++e) v[e] = ps[e];
+            } else {
+                acc.sync();
+#pragma unroll
+                for (int e = 0; e < EH; ++e) {
+                    const int q = in_pos<M, EH, 0>(e, t);
+                    acc(2 * q) = ps[2 * e];
+                    acc(2 * q + 1) = ps[2 * e + 1];
+                }
+                acc.sync();
+#pragma unroll
+                for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+            }
+            fft_pencil<N, E, -1, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
             C* dst = a.out + row * N;
 #pragma unroll
             for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];

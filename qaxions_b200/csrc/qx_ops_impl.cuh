@@ -198,7 +198,7 @@ struct TmaGeom {
     size_t tile_bytes;
 };
 
-template <int NN, typename R, int PW>
+template <int NN, typename R, int PW, int TXF>
 static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
     using C = cx_t<R>;
     TmaGeom g;
@@ -208,9 +208,9 @@ static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
     // 512^3 against 16 columns / deeper rings)
     int tx = want_tx > 0 ? want_tx : 8;
     while (tx > PW && ((X % tx) || (tx / PW) * g.T > tma_max_threads<PW>())) tx >>= 1;
-    if (tma_tx_fixed<NN>() > 0) {  // compiled-in tile width
-        tx = tma_tx_fixed<NN>();
-        if ((X % tx) || (tx / PW) * g.T > tma_max_threads<PW>()) throw std::logic_error("TMA tile width does not fit");
+    if (TXF > 0) {  // compiled-in tile width
+        tx = TXF;
+        if ((X % tx) || (tx / PW) * g.T > 512) throw std::logic_error("TMA tile width does not fit");
     }
     g.TX = tx;
     g.box = NN <= 256 ? NN : 256;
@@ -241,10 +241,10 @@ template <typename R, int OP> static bool use_df(const typename Ops<R>::SP& a) {
 }
 
 // Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
-template <int NN, typename R, int OP, int PW, bool DF>
+template <int NN, typename R, int OP, int PW, bool DF, int TXF>
 static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                          const Tune& tu, cudaStream_t st) {
-    const TmaGeom g = tma_geom<NN, R, PW>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
+    const TmaGeom g = tma_geom<NN, R, PW, TXF>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
     TArgs<R> s;
     s.tw = a.tw;
     s.tw_lo = a.tw_lo;
@@ -267,7 +267,7 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.partial = a.partial;
     s.err = a.err;
     const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim);
-    auto kern = k_pencil_tma<NN, R, OP, PW, DF>;
+    auto kern = k_pencil_tma<NN, R, OP, PW, DF, TXF>;
     const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
@@ -285,14 +285,33 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     return grid;
 }
 
+// tile columns: tu.la_tx (last axis) / tu.y_tx (y passes) when 8 or 16, else 8
+// (FP32 16 is compiled for N >= 64: it streams z pencils faster, but at 512^3
+// the FP32 passes are compute-bound and one 512-thread block per SM loses
+// more than the wider rows gain).  Grids N < 16 choose at run time.
+template <int NN, typename R, int OP, int PW, bool DF>
+static long launch_tma_tx(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
+                          const Tune& tu, cudaStream_t st) {
+    if constexpr (NN < 16) {
+        return launch_tma_e<NN, R, OP, PW, DF, 0>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    } else {
+        const int want = (pencil_dim == 2 || outer == 1) ? tu.la_tx : tu.y_tx;
+        const int tx = want == 8 || want == 16 ? want : 8;
+        if constexpr (sizeof(R) == 4 && NN >= 64) {
+            if (tx == 16) return launch_tma_e<NN, R, OP, PW, DF, 16>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+        }
+        return launch_tma_e<NN, R, OP, PW, DF, 8>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    }
+}
+
 // pencils per thread: tu.pw, default 2 in the FP32 form (paired columns), 1 in FP64
 template <int NN, typename R, int OP, bool DF>
 static long launch_tma_df(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                           const Tune& tu, cudaStream_t st) {
     if constexpr (sizeof(R) == 4) {
-        if (tu.pw != 1) return launch_tma_e<NN, R, OP, 2, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+        if (tu.pw != 1) return launch_tma_tx<NN, R, OP, 2, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
     }
-    return launch_tma_e<NN, R, OP, 1, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+    return launch_tma_tx<NN, R, OP, 1, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
 }
 
 template <int NN, typename R, int OP>

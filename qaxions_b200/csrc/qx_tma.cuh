@@ -112,9 +112,17 @@ template <int N, typename R, int PW> __host__ __device__ constexpr int tma_e() {
 // blocks up to 256 threads with two blocks per SM
 template <int PW> __host__ __device__ constexpr int tma_max_threads() { return PW == 2 ? 256 : 512; }
 template <int PW> __host__ __device__ constexpr int tma_min_blocks() { return PW == 2 ? 2 : 1; }
-// tile columns: 8 (64-byte FP32 / 128-byte FP64 rows), fixed at compile time so
-// shared-memory addresses fold to constants; smaller grids pick at run time
-template <int N> __host__ __device__ constexpr int tma_tx_fixed() { return N >= 16 ? 8 : 0; }
+// Tile columns TXF: 8 or 16, fixed at compile time so shared-memory addresses
+// fold to constants (0: chosen at run time, grids N < 16).  Rows of a tile
+// are TXF * sizeof(complex) bytes of one HBM row; at the 2 MB stride of a z
+// pencil, 128-byte rows (FP32 TXF = 16, FP64 TXF = 8) stream at nearly the
+// rate of contiguous copies, 64-byte rows at about half of it.
+template <int N, typename R, int PW, int TXF> __host__ __device__ constexpr int tma_block_threads() {
+    return TXF > 0 ? (TXF / PW) * (N / tma_e<N, R, PW>()) : tma_max_threads<PW>();
+}
+template <int N, typename R, int PW, int TXF> __host__ __device__ constexpr int tma_block_min() {
+    return TXF > 0 ? (tma_block_threads<N, R, PW, TXF>() <= 256 ? 2 : 1) : tma_min_blocks<PW>();
+}
 
 __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
 
@@ -142,9 +150,10 @@ template <typename R> struct TArgs {
     int* err;            // set to 1 when a wait timed out
 };
 
-// blockDim = (TX / PW, N / E): thread (c, t) owns columns x0 + PW c + h (h < PW)
-template <int N, typename R, int OP, int PW, bool DF>
-__global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
+// blockDim = (TX / PW, N / E): thread (c, t) owns columns x0 + PW c + h (h < PW);
+// TX = TXF when TXF > 0
+template <int N, typename R, int OP, int PW, bool DF, int TXF>
+__global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_block_min<N, R, PW, TXF>()))
     k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
     using P = pencil_val_t<PW, C>;
@@ -154,7 +163,7 @@ __global__ void __launch_bounds__(tma_max_threads<PW>(), tma_min_blocks<PW>())
     __shared__ __align__(8) uint64_t mbar[8];
     __shared__ int s_abort;
     __shared__ double red[32];
-    const int TX = tma_tx_fixed<N>() > 0 ? tma_tx_fixed<N>() : s.TX;
+    const int TX = TXF > 0 ? TXF : s.TX;
     const int TG = TX / PW;  // pencil groups per tile row
     const int c = threadIdx.x, t = threadIdx.y;
     const int tid = c + TG * t;
