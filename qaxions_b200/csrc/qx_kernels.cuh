@@ -177,7 +177,8 @@ __device__ double block_reduce(double v, double* red) {
 
 // ---------------------------------------------------------------------------
 // x passes (contiguous rows).  blockDim = (T, P): T = qx_row_threads(N)
-// threads per row, P rows per block.  Dynamic smem: P * row_smem_elems(N) C.
+// threads per row, P rows per block; persistent grid, each warp loops over its
+// rows.  Dynamic smem: twiddle tables (x_table_elems) + P * row_smem_elems(N) C.
 // ---------------------------------------------------------------------------
 
 template <typename R> struct XArgs {
@@ -196,6 +197,42 @@ template <typename R> struct XArgs {
     double scale;           // applied after an inverse c2c (1/S when requested)
 };
 
+// shared twiddle tables of a row pass (complex elements): N-point table, its
+// low part (FP32 only), N/2-point table
+template <int N, typename R> __host__ __device__ constexpr int x_table_elems() {
+    return N + (sizeof(R) == 4 ? N : 0) + N / 2;
+}
+
+template <typename C> struct XTabs {
+    const C* N;
+    const C* N_lo;
+    const C* M;
+};
+
+// Copy the twiddle tables into shared memory once per (persistent) block and
+// return the row buffer of the calling thread's row slot.
+template <int N, typename R>
+__device__ __forceinline__ cx_t<R>* x_setup(const XArgs<R>& a, unsigned char* smem, XTabs<cx_t<R>>& tb) {
+    using C = cx_t<R>;
+    C* tN = reinterpret_cast<C*>(smem);
+    C* tNl = tN + N;
+    C* tM = tNl + (sizeof(R) == 4 ? N : 0);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nthr = blockDim.x * blockDim.y;
+    for (int i = tid; i < N; i += nthr) {
+        tN[i] = a.twN[i];
+        if constexpr (sizeof(R) == 4) tNl[i] = a.twN_lo[i];
+    }
+    for (int i = tid; i < N / 2; i += nthr) tM[i] = a.twM[i];
+    __syncthreads();
+    tb = XTabs<C>{tN, sizeof(R) == 4 ? tNl : tN, tM};
+    return tN + x_table_elems<N, R>() + threadIdx.y * row_smem_elems(N);
+}
+
+// first row of this thread's row slot and the row stride of the grid
+__device__ __forceinline__ long x_row0() { return (long)blockIdx.x * blockDim.y + threadIdx.y; }
+__device__ __forceinline__ long x_row_step() { return (long)gridDim.x * blockDim.y; }
+
 enum XFwdMode { XF_PLAIN = 0, XF_KICK = 1 };
 
 // forward c2c along x; optional kick by V first.  (Field::kick + first FFT pass)
@@ -204,22 +241,25 @@ __global__ void __launch_bounds__(256, 3) k_x_fwd(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    XTabs<C> tb;
+    C* sm = x_setup<N, R>(a, smem_raw, tb);
     const int t = threadIdx.x;
-    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
-    const C* src = a.in + row * N;
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int p = in_pos<N, E, 0>(e, t);
-        v[e] = src[p];
-        if constexpr (MODE == XF_KICK) v[e] = kick1<R>(v[e], a.Vin[row * N + p], a.dt);
-    }
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    fft_pencil<N, E, -1>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
-    C* dst = a.out + row * N;
+    for (long row = x_row0(); row < a.rows; row += x_row_step()) {
+        acc.sync();  // this slot's previous row is done with the buffer
+        const C* src = a.in + row * N;
+        C v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
+        for (int e = 0; e < E; ++e) {
+            const int p = in_pos<N, E, 0>(e, t);
+            v[e] = src[p];
+            if constexpr (MODE == XF_KICK) v[e] = kick1<R>(v[e], a.Vin[row * N + p], a.dt);
+        }
+        fft_pencil<N, E, -1>(v, acc, t, tw_src<true>(tb.N, tb.N_lo));
+        C* dst = a.out + row * N;
+#pragma unroll
+        for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
+    }
 }
 
 // r2c post-processing of one row held in smem (Z[k], k < M) -> packed X row.
@@ -240,7 +280,7 @@ __device__ __forceinline__ void r2c_post_store(RowAcc<cx_t<R>>& acc, int t, cx_t
         } else {
             const C B = cconj(acc(M - k));
             const C s = cadd(A, B), d = csub(A, B);
-            const C w = __ldg(&twN[k]);
+            const C w = twN[k];
             // -i * w * d
             const C wd = cmul(w, d);
             x = mk<C>(R(0.5) * (s.x + wd.y), R(0.5) * (s.y - wd.x));
@@ -259,52 +299,56 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
-    const int t = threadIdx.x;
-    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
     constexpr bool PAIRED = row_paired<N>();
-    const C* src = a.in + row * N;
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = src[out_pos<N, E>(e, t)];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    XTabs<C> tb;
+    C* sm = x_setup<N, R>(a, smem_raw, tb);
+    const int t = threadIdx.x;
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    ifft_pencil_rev<N, E, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
-    const R sc = (R)a.scale;
-    C* dst = a.out + row * N;
+    for (long row = x_row0(); row < a.rows; row += x_row_step()) {
+        acc.sync();
+        const C* src = a.in + row * N;
+        C v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cscale(v[e], sc);
-    if constexpr (PAIRED) {
+        for (int e = 0; e < E; ++e) v[e] = src[out_pos<N, E>(e, t)];
+        ifft_pencil_rev<N, E, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(tb.N, tb.N_lo));
+        const R sc = (R)a.scale;
+        C* dst = a.out + row * N;
 #pragma unroll
-        for (int e = 0; e < EH; ++e)
-            store_pair(dst, in_pos<M, EH, 0>(e, t), v[row_pair_idx<N>(e, 0)], v[row_pair_idx<N>(e, 1)]);
-    } else {
-#pragma unroll
-        for (int e = 0; e < E; ++e) dst[in_pos<N, E, 0>(e, t)] = v[e];
-    }
-    if constexpr (MODE == XI_R2C) {
-        const R pr = (R)a.pref, rm = (R)a.rho_mean;
-        auto src_of = [&](const C& u) { return pr * (u.x * u.x + u.y * u.y - rm); };
-        C z[EH];  // (rho[2q], rho[2q+1]), q = in_pos<M, EH, 0>(e, t)
+        for (int e = 0; e < E; ++e) v[e] = cscale(v[e], sc);
         if constexpr (PAIRED) {
 #pragma unroll
-            for (int e = 0; e < EH; ++e) z[e] = mk<C>(src_of(v[row_pair_idx<N>(e, 0)]), src_of(v[row_pair_idx<N>(e, 1)]));
+            for (int e = 0; e < EH; ++e)
+                store_pair(dst, in_pos<M, EH, 0>(e, t), v[row_pair_idx<N>(e, 0)], v[row_pair_idx<N>(e, 1)]);
         } else {
-            // stage the real source in smem (as R[N] over the same buffer)
-            R* rs = reinterpret_cast<R*>(sm);
-            acc.sync();
 #pragma unroll
-            for (int e = 0; e < E; ++e) rs[in_pos<N, E, 0>(e, t)] = src_of(v[e]);
-            acc.sync();
-#pragma unroll
-            for (int e = 0; e < EH; ++e) z[e] = reinterpret_cast<const C*>(rs)[in_pos<M, EH, 0>(e, t)];
+            for (int e = 0; e < E; ++e) dst[in_pos<N, E, 0>(e, t)] = v[e];
         }
-        fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
-        acc.sync();
+        if constexpr (MODE == XI_R2C) {
+            const R pr = (R)a.pref, rm = (R)a.rho_mean;
+            auto src_of = [&](const C& u) { return pr * (u.x * u.x + u.y * u.y - rm); };
+            C z[EH];  // (rho[2q], rho[2q+1]), q = in_pos<M, EH, 0>(e, t)
+            if constexpr (PAIRED) {
 #pragma unroll
-        for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
-        acc.sync();
-        r2c_post_store<N, R>(acc, t, a.vh + row * M, a.twN);
+                for (int e = 0; e < EH; ++e)
+                    z[e] = mk<C>(src_of(v[row_pair_idx<N>(e, 0)]), src_of(v[row_pair_idx<N>(e, 1)]));
+            } else {
+                // stage the real source in smem (as R[N] over the same buffer)
+                R* rs = reinterpret_cast<R*>(sm);
+                acc.sync();
+#pragma unroll
+                for (int e = 0; e < E; ++e) rs[in_pos<N, E, 0>(e, t)] = src_of(v[e]);
+                acc.sync();
+#pragma unroll
+                for (int e = 0; e < EH; ++e) z[e] = reinterpret_cast<const C*>(rs)[in_pos<M, EH, 0>(e, t)];
+            }
+            fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(tb.M, tb.M));
+            acc.sync();
+#pragma unroll
+            for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
+            acc.sync();
+            r2c_post_store<N, R>(acc, t, a.vh + row * M, tb.N);
+        }
     }
 }
 
@@ -319,30 +363,32 @@ __global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    XTabs<C> tb;
+    C* sm = x_setup<N, R>(a, smem_raw, tb);
     const int t = threadIdx.x;
-    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
-    C z[EH];
-    const R pr = (R)a.pref, rm = (R)a.rho_mean;
-#pragma unroll
-    for (int e = 0; e < EH; ++e) {
-        const int q = in_pos<M, EH, 0>(e, t);
-        if constexpr (SRC == XR_DENSITY) {
-            C p0, p1;
-            load_pair(a.in + row * N, q, p0, p1);
-            z[e] = mk<C>(pr * (p0.x * p0.x + p0.y * p0.y - rm), pr * (p1.x * p1.x + p1.y * p1.y - rm));
-        } else {
-            const C pair = reinterpret_cast<const C*>(a.Vin + row * N)[q];
-            z[e] = pair;
-        }
-    }
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
-    acc.sync();
+    const R pr = (R)a.pref, rm = (R)a.rho_mean;
+    for (long row = x_row0(); row < a.rows; row += x_row_step()) {
+        acc.sync();
+        C z[EH];
 #pragma unroll
-    for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
-    acc.sync();
-    r2c_post_store<N, R>(acc, t, a.vh + row * M, a.twN);
+        for (int e = 0; e < EH; ++e) {
+            const int q = in_pos<M, EH, 0>(e, t);
+            if constexpr (SRC == XR_DENSITY) {
+                C p0, p1;
+                load_pair(a.in + row * N, q, p0, p1);
+                z[e] = mk<C>(pr * (p0.x * p0.x + p0.y * p0.y - rm), pr * (p1.x * p1.x + p1.y * p1.y - rm));
+            } else {
+                z[e] = reinterpret_cast<const C*>(a.Vin + row * N)[q];
+            }
+        }
+        fft_pencil<M, EH, -1>(z, acc, t, tw_src<false>(tb.M, tb.M));
+        acc.sync();
+#pragma unroll
+        for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
+        acc.sync();
+        r2c_post_store<N, R>(acc, t, a.vh + row * M, tb.N);
+    }
 }
 
 enum XC2RFlags {
@@ -362,75 +408,79 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     constexpr int EH = E / 2;
     constexpr int T = qx_row_threads(N);
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw) + threadIdx.y * row_smem_elems(N);
+    XTabs<C> tb;
+    C* sm = x_setup<N, R>(a, smem_raw, tb);
     const int t = threadIdx.x;
-    const long row = (long)blockIdx.x * blockDim.y + threadIdx.y;
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    const C* hrow = a.vh + row * M;
+    for (long row = x_row0(); row < a.rows; row += x_row_step()) {
+        acc.sync();
+        const C* hrow = a.vh + row * M;
 #pragma unroll
-    for (int i = 0; i < M / T; ++i) acc(t + i * T) = hrow[t + i * T];
-    acc.sync();
-    C z[EH];
-#pragma unroll
-    for (int e = 0; e < EH; ++e) {
-        const int k = out_pos<M, EH>(e, t);
-        const C X = acc(k);
-        if (k == 0) {
-            // X[0] = Re col0, X[N/2] = Im col0
-            z[e] = mk<C>(X.x + X.y, X.x - X.y);
-        } else {
-            const C B = cconj(acc(M - k));
-            const C s = cadd(X, B), d = csub(X, B);
-            const C w = cconj(__ldg(&a.twN[k]));  // W_N^{-k}
-            const C wd = cmul(w, d);
-            z[e] = mk<C>(s.x - wd.y, s.y + wd.x);  // s + i*wd
-        }
-    }
-    ifft_pencil_rev<M, EH>(z, acc, t, tw_src<false>(a.twM, a.twM_lo));
-    // z at in_pos<M, EH, 0> q holds (V[2q], V[2q+1])
-    if constexpr (FLAGS & XC_WRITE_V) {
-        C* vrow = reinterpret_cast<C*>(a.Vout + row * N);
-#pragma unroll
-        for (int e = 0; e < EH; ++e) vrow[in_pos<M, EH, 0>(e, t)] = z[e];
-    }
-    if constexpr (FLAGS & XC_KICK) {
-        constexpr bool PAIRED = row_paired<N>();
-        C ps[E];  // kicked psi: position 2q+h in ps[row_pair_idx<N>(e, h)]
+        for (int i = 0; i < M / T; ++i) acc(t + i * T) = hrow[t + i * T];
+        acc.sync();
+        C z[EH];
 #pragma unroll
         for (int e = 0; e < EH; ++e) {
-            C p0, p1;
-            load_pair(a.in + row * N, in_pos<M, EH, 0>(e, t), p0, p1);
-            ps[row_pair_idx<N>(e, 0)] = kick1<R>(p0, z[e].x, a.dt);
-            ps[row_pair_idx<N>(e, 1)] = kick1<R>(p1, z[e].y, a.dt);
+            const int k = out_pos<M, EH>(e, t);
+            const C X = acc(k);
+            if (k == 0) {
+                // X[0] = Re col0, X[N/2] = Im col0
+                z[e] = mk<C>(X.x + X.y, X.x - X.y);
+            } else {
+                const C B = cconj(acc(M - k));
+                const C s = cadd(X, B), d = csub(X, B);
+                const C w = cconj(tb.N[k]);  // W_N^{-k}
+                const C wd = cmul(w, d);
+                z[e] = mk<C>(s.x - wd.y, s.y + wd.x);  // s + i*wd
+            }
         }
-        if constexpr (FLAGS & XC_WRITE_PSI) {
+        ifft_pencil_rev<M, EH>(z, acc, t, tw_src<false>(tb.M, tb.M));
+        // z at in_pos<M, EH, 0> q holds (V[2q], V[2q+1])
+        if constexpr (FLAGS & XC_WRITE_V) {
+            C* vrow = reinterpret_cast<C*>(a.Vout + row * N);
+#pragma unroll
+            for (int e = 0; e < EH; ++e) vrow[in_pos<M, EH, 0>(e, t)] = z[e];
+        }
+        if constexpr (FLAGS & XC_KICK) {
+            constexpr bool PAIRED = row_paired<N>();
+            C ps[E];  // kicked psi: position 2q+h in ps[row_pair_idx<N>(e, h)]
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
-                store_pair(a.out + row * N, in_pos<M, EH, 0>(e, t), ps[row_pair_idx<N>(e, 0)], ps[row_pair_idx<N>(e, 1)]);
+                C p0, p1;
+                load_pair(a.in + row * N, in_pos<M, EH, 0>(e, t), p0, p1);
+                ps[row_pair_idx<N>(e, 0)] = kick1<R>(p0, z[e].x, a.dt);
+                ps[row_pair_idx<N>(e, 1)] = kick1<R>(p1, z[e].y, a.dt);
             }
-        }
-        if constexpr (FLAGS & XC_FWD) {
-            C v[E];
-            if constexpr (PAIRED) {
-                // already in the paired stage-0 input order
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = ps[e];
-            } else {
-                acc.sync();
+            if constexpr (FLAGS & XC_WRITE_PSI) {
 #pragma unroll
                 for (int e = 0; e < EH; ++e) {
-                    const int q = in_pos<M, EH, 0>(e, t);
-                    acc(2 * q) = ps[2 * e];
-                    acc(2 * q + 1) = ps[2 * e + 1];
+                    store_pair(a.out + row * N, in_pos<M, EH, 0>(e, t), ps[row_pair_idx<N>(e, 0)],
+                               ps[row_pair_idx<N>(e, 1)]);
                 }
-                acc.sync();
-#pragma unroll
-                for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
             }
-            fft_pencil<N, E, -1, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(a.twN, a.twN_lo));
-            C* dst = a.out + row * N;
+            if constexpr (FLAGS & XC_FWD) {
+                C v[E];
+                if constexpr (PAIRED) {
+                    // already in the paired stage-0 input order
 #pragma unroll
-            for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
+                    for (int e = 0; e < E; ++e) v[e] = ps[e];
+                } else {
+                    acc.sync();
+#pragma unroll
+                    for (int e = 0; e < EH; ++e) {
+                        const int q = in_pos<M, EH, 0>(e, t);
+                        acc(2 * q) = ps[2 * e];
+                        acc(2 * q + 1) = ps[2 * e + 1];
+                    }
+                    acc.sync();
+#pragma unroll
+                    for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
+                }
+                fft_pencil<N, E, -1, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(tb.N, tb.N_lo));
+                C* dst = a.out + row * N;
+#pragma unroll
+                for (int e = 0; e < E; ++e) dst[out_pos<N, E>(e, t)] = v[e];
+            }
         }
     }
 }

@@ -69,15 +69,46 @@ static int x_rows_per_block(int N, long rows, int want) {
     return 1;
 }
 
+static int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cache[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 1;
+    }
+    return cache[dev];
+}
+
 template <typename R, int NN, typename K>
 static void launch_x(K kernel, const XArgs<R>& x, int P, cudaStream_t st) {
     using C = cx_t<R>;
     const int T = qx_row_threads(NN);
-    const size_t smem = (size_t)P * row_smem_elems(NN) * sizeof(C);
+    const size_t smem = ((size_t)x_table_elems<NN, R>() + (size_t)P * row_smem_elems(NN)) * sizeof(C);
     set_smem(kernel, smem);
+    // persistent grid: as many blocks as fit on the device at once (the
+    // twiddle tables are staged once per block), at most one per P rows
+    static const void* cache_k[32] = {nullptr};
+    static int cache_bps[32] = {0};
+    int bps = 0;
+    for (int i = 0; i < 32 && cache_k[i]; ++i)
+        if (cache_k[i] == (const void*)kernel) bps = cache_bps[i];
+    if (!bps) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, T * P, smem) != cudaSuccess || bps < 1) bps = 1;
+        for (int i = 0; i < 32; ++i)
+            if (!cache_k[i]) {
+                cache_k[i] = (const void*)kernel;
+                cache_bps[i] = bps;
+                break;
+            }
+    }
+    const long blocks = x.rows / P;
+    long grid = (long)sm_count() * bps;
+    if (grid > blocks) grid = blocks;
     dim3 blk(T, P);
-    dim3 grd((unsigned)(x.rows / P));
-    kernel<<<grd, blk, smem, st>>>(x);
+    kernel<<<(unsigned)grid, blk, smem, st>>>(x);
     QX_LAUNCH_CHECK();
 }
 
@@ -179,18 +210,6 @@ static CUtensorMap make_tmap(const void* base, int X, int N, int NZ, int TX, int
     return tm;
 }
 
-static int sm_count() {
-    static int cache[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) dev = 0;
-    if (!cache[dev]) {
-        int n = 0;
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        cache[dev] = n > 0 ? n : 1;
-    }
-    return cache[dev];
-}
 
 // Launch geometry of a TMA pencil pass.
 struct TmaGeom {
