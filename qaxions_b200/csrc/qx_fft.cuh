@@ -226,8 +226,16 @@ template <int L, int E> __device__ __forceinline__ int out_pos(int e, int t) {
     return t + (e / r) * T + (e % r) * (L / r);
 }
 
-// Twiddle sources: a table of exp(-2 pi i j/L) (global or a shared-memory
-// copy), or a double-float pair of tables hi + lo (lo = exact - hi), which
+// Twiddle tables are stage-major: stage s >= 1 (span Ns, radix r) keeps its
+// (r-1) Ns twiddles w_L^(k m L/(Ns r)) at (Ns - r0) + (m-1) Ns + k, so lanes
+// with consecutive butterfly columns k read consecutive words (no bank
+// conflicts when staged in shared memory); a table has L - r0 entries.
+__host__ __device__ constexpr int qx_tw_index(int L, int Ns, int m, int k) {
+    return (Ns - qx_radix(L, 0)) + (m - 1) * Ns + k;
+}
+
+// Twiddle sources: a stage-major table (global or a shared-memory copy), or a
+// double-float pair of such tables hi + lo (lo = exact - hi), which
 // applies each twiddle to twice the working precision.  A twiddle table is
 // applied with the same values at every time step, so its rounding error
 // would otherwise compound over the steps for modes whose forward and
@@ -283,9 +291,8 @@ __device__ __forceinline__ void fft_stages(C (&v)[E], Acc& acc, int t, const TW&
             const int j = stage_j<L, E, s, J0>(b, t);
             if constexpr (Ns > 1) {
                 const int k = j % Ns;
-                constexpr int stw = L / (Ns * r);
 #pragma unroll
-                for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<SIGN>(v[b * r + m], tw, k * m * stw);
+                for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<SIGN>(v[b * r + m], tw, qx_tw_index(L, Ns, m, k));
             }
             dft<r, SIGN>(&v[b * r]);
         }
@@ -355,9 +362,8 @@ __device__ __forceinline__ void ifft_rev_stages(C (&v)[E], Acc& acc, int t, cons
         dft<r, +1>(&v[b * r]);
         if constexpr (Ns > 1) {
             const int k = stage_j<L, E, s, J0>(b, t) % Ns;
-            constexpr int stw = L / (Ns * r);
 #pragma unroll
-            for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<+1>(v[b * r + m], tw, k * m * stw);
+            for (int m = 1; m < r; ++m) v[b * r + m] = tw_mul<+1>(v[b * r + m], tw, qx_tw_index(L, Ns, m, k));
         }
     }
     if constexpr (s > 0) {

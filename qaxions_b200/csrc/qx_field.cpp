@@ -203,6 +203,7 @@ static typename Ops<R>::XP xp0(const Geometry& g, const TwTables<typename Ops<R>
     a.twM = tw.M;
     a.twN_lo = tw.N_lo;
     a.twM_lo = tw.M_lo;
+    a.twNn = tw.N_nat;
     a.rows = g.rows;
     a.scale = 1.0;
     a.pref = 1.0;
@@ -330,15 +331,23 @@ class FieldT final : public Field {
         QX_CUDA(cudaMemsetAsync(errbuf_.p, 0, sizeof(int), st_));
         auto tN = twiddles<C>(cfg.N), tM = twiddles<C>(cfg.N / 2);
         auto tNl = twiddles_lo<C>(cfg.N, tN), tMl = twiddles_lo<C>(cfg.N / 2, tM);
-        twN_.alloc(sizeof(C) * tN.size());
-        twM_.alloc(sizeof(C) * tM.size());
-        twNl_.alloc(sizeof(C) * tN.size());
-        twMl_.alloc(sizeof(C) * tM.size());
-        QX_CUDA(cudaMemcpy(twN_.p, tN.data(), sizeof(C) * tN.size(), cudaMemcpyHostToDevice));
-        QX_CUDA(cudaMemcpy(twM_.p, tM.data(), sizeof(C) * tM.size(), cudaMemcpyHostToDevice));
-        QX_CUDA(cudaMemcpy(twNl_.p, tNl.data(), sizeof(C) * tN.size(), cudaMemcpyHostToDevice));
-        QX_CUDA(cudaMemcpy(twMl_.p, tMl.data(), sizeof(C) * tM.size(), cudaMemcpyHostToDevice));
-        tw_ = TwTables<C>{twN_.as<C>(), twM_.as<C>(), twNl_.as<C>(), twMl_.as<C>()};
+        // stage-major FFT tables (same values, reordered per stage)
+        std::vector<C> sN(tN.size(), C{0, 0}), sM(tM.size(), C{0, 0}), sNl(tN.size(), C{0, 0}),
+            sMl(tM.size(), C{0, 0});
+        Ops<R>::stage_twiddles(tN.data(), cfg.N, sN.data());
+        Ops<R>::stage_twiddles(tNl.data(), cfg.N, sNl.data());
+        Ops<R>::stage_twiddles(tM.data(), cfg.N / 2, sM.data());
+        Ops<R>::stage_twiddles(tMl.data(), cfg.N / 2, sMl.data());
+        auto upload = [&](DevBuf& b, const std::vector<C>& h) {
+            b.alloc(sizeof(C) * h.size());
+            QX_CUDA(cudaMemcpy(b.p, h.data(), sizeof(C) * h.size(), cudaMemcpyHostToDevice));
+        };
+        upload(twN_, sN);
+        upload(twM_, sM);
+        upload(twNl_, sNl);
+        upload(twMl_, sMl);
+        upload(twNn_, tN);
+        tw_ = TwTables<C>{twN_.as<C>(), twM_.as<C>(), twNl_.as<C>(), twMl_.as<C>(), twNn_.as<C>()};
         QX_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
@@ -925,7 +934,7 @@ class FieldT final : public Field {
 
   private:
     int device_ = 0;
-    DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, red_, redout_, errbuf_;
+    DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, twNn_, red_, redout_, errbuf_;
     TwTables<C> tw_{};
     int* err_ = nullptr;
     DevBuf mpsi_, mvh_, kin_, specP_, specC_, stage_;

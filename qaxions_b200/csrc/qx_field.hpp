@@ -64,13 +64,16 @@ struct Geometry {
     long fftw_ksites() const { return rows * (N / 2 + 1); }
 };
 
-// device twiddle tables exp(-2 pi i j/L) for L = N and N/2, with the low
-// parts (exact - table) used by the FP32 form's double-float twiddles
+// device twiddle tables for L = N and N/2: the FFT passes read stage-major
+// tables (Ops::stage_twiddles), with the low parts (exact - table) used by the
+// FP32 form's double-float twiddles; the r2c/c2r pre/post-processing reads the
+// natural-order table exp(-2 pi i k/N)
 template <typename C> struct TwTables {
     const C* N;
     const C* M;
     const C* N_lo;
     const C* M_lo;
+    const C* N_nat;
 };
 
 template <typename R>

@@ -187,26 +187,28 @@ template <typename R> struct XArgs {
     cx_t<R>* vh;            // packed half rows of N/2
     const R* Vin;           // real rows of N (potential for the kick / r2c source)
     R* Vout;                // real rows of N
-    const cx_t<R>* twN;     // exp(-2 pi i j/N), j < N
-    const cx_t<R>* twM;     // exp(-2 pi i j/(N/2)), j < N/2
+    const cx_t<R>* twN;     // stage-major N-point FFT twiddles (qx_tw_index)
+    const cx_t<R>* twM;     // stage-major N/2-point FFT twiddles
     const cx_t<R>* twN_lo;  // exact - twN (double-float twiddles of the FP32 form)
     const cx_t<R>* twM_lo;
+    const cx_t<R>* twNn;    // natural-order exp(-2 pi i k/N), k < N/2 (r2c/c2r)
     long rows;
     double dt;              // kick time step
     double pref, rho_mean;  // r2c source pref*(|psi|^2 - rho_mean)
     double scale;           // applied after an inverse c2c (1/S when requested)
 };
 
-// shared twiddle tables of a row pass (complex elements): N-point table, its
-// low part (FP32 only), N/2-point table
+// shared twiddle tables of a row pass (complex elements): N-point FFT table,
+// its low part (FP32 only), N/2-point FFT table, natural-order k < N/2 table
 template <int N, typename R> __host__ __device__ constexpr int x_table_elems() {
-    return N + (sizeof(R) == 4 ? N : 0) + N / 2;
+    return N + (sizeof(R) == 4 ? N : 0) + N / 2 + N / 2;
 }
 
 template <typename C> struct XTabs {
     const C* N;
     const C* N_lo;
     const C* M;
+    const C* Nn;
 };
 
 // Copy the twiddle tables into shared memory once per (persistent) block and
@@ -217,15 +219,19 @@ __device__ __forceinline__ cx_t<R>* x_setup(const XArgs<R>& a, unsigned char* sm
     C* tN = reinterpret_cast<C*>(smem);
     C* tNl = tN + N;
     C* tM = tNl + (sizeof(R) == 4 ? N : 0);
+    C* tNn = tM + N / 2;
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
     const int nthr = blockDim.x * blockDim.y;
     for (int i = tid; i < N; i += nthr) {
         tN[i] = a.twN[i];
         if constexpr (sizeof(R) == 4) tNl[i] = a.twN_lo[i];
     }
-    for (int i = tid; i < N / 2; i += nthr) tM[i] = a.twM[i];
+    for (int i = tid; i < N / 2; i += nthr) {
+        tM[i] = a.twM[i];
+        tNn[i] = a.twNn[i];
+    }
     __syncthreads();
-    tb = XTabs<C>{tN, sizeof(R) == 4 ? tNl : tN, tM};
+    tb = XTabs<C>{tN, sizeof(R) == 4 ? tNl : tN, tM, tNn};
     return tN + x_table_elems<N, R>() + threadIdx.y * row_smem_elems(N);
 }
 
@@ -347,7 +353,7 @@ __global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
 #pragma unroll
             for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
             acc.sync();
-            r2c_post_store<N, R>(acc, t, a.vh + row * M, tb.N);
+            r2c_post_store<N, R>(acc, t, a.vh + row * M, tb.Nn);
         }
     }
 }
@@ -387,7 +393,7 @@ __global__ void __launch_bounds__(256, 3) k_x_r2c(XArgs<R> a) {
 #pragma unroll
         for (int e = 0; e < EH; ++e) acc(out_pos<M, EH>(e, t)) = z[e];
         acc.sync();
-        r2c_post_store<N, R>(acc, t, a.vh + row * M, tb.N);
+        r2c_post_store<N, R>(acc, t, a.vh + row * M, tb.Nn);
     }
 }
 
@@ -429,7 +435,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
             } else {
                 const C B = cconj(acc(M - k));
                 const C s = cadd(X, B), d = csub(X, B);
-                const C w = cconj(tb.N[k]);  // W_N^{-k}
+                const C w = cconj(tb.Nn[k]);  // W_N^{-k}
                 const C wd = cmul(w, d);
                 z[e] = mk<C>(s.x - wd.y, s.y + wd.x);  // s + i*wd
             }

@@ -27,8 +27,9 @@ template <typename R> struct Ops {
     using C = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
     struct XP {
         const C* in; C* out; C* vh; const R* Vin; R* Vout;
-        const C* twN; const C* twM;
+        const C* twN; const C* twM;        // stage-major FFT twiddles (N- and N/2-point)
         const C* twN_lo; const C* twM_lo;  // low parts (exact - table), FP32 double-float twiddles
+        const C* twNn;                     // natural-order exp(-2 pi i k/N), k < N/2 (r2c/c2r)
         long rows; double dt, pref, rho_mean, scale;
     };
     struct SP {
@@ -45,6 +46,9 @@ template <typename R> struct Ops {
     // last-axis pass; returns the number of blocks (partials written for OP_KIN)
     static long la_pass(int N, const SP& s, int op, const Tune& tu, cudaStream_t st);
     static long la_blocks(int N, int X, int dim, int op, const Tune& tu);
+    // stage-major FFT twiddle table of length L from the natural-order table
+    // nat[j] = exp(-2 pi i j/L) (entries beyond L - r0 are left as they are)
+    static void stage_twiddles(const C* nat, int L, C* out);
 };
 
 }  // namespace qx

@@ -46,7 +46,7 @@ static void set_smem(K kernel, size_t bytes) {
 template <typename R> static XArgs<R> to_x(const typename Ops<R>::XP& a) {
     XArgs<R> x;
     x.in = a.in; x.out = a.out; x.vh = a.vh; x.Vin = a.Vin; x.Vout = a.Vout;
-    x.twN = a.twN; x.twM = a.twM; x.twN_lo = a.twN_lo; x.twM_lo = a.twM_lo;
+    x.twN = a.twN; x.twM = a.twM; x.twN_lo = a.twN_lo; x.twM_lo = a.twM_lo; x.twNn = a.twNn;
     x.rows = a.rows; x.dt = a.dt; x.pref = a.pref;
     x.rho_mean = a.rho_mean; x.scale = a.scale;
     return x;
@@ -56,6 +56,16 @@ template <typename R> static SArgs<R> to_s(const typename Ops<R>::SP& a) {
     s.a = a.a; s.tw = a.tw; s.tw_lo = a.tw_lo; s.X = a.X; s.dim = a.dim; s.N = a.N; s.phase_fac = a.phase_fac;
     s.scale = a.scale; s.pois_c = a.pois_c; s.pois_g0 = a.pois_g0; s.partial = a.partial;
     return s;
+}
+
+template <typename R>
+void Ops<R>::stage_twiddles(const C* nat, int L, C* out) {
+    const int S = qx_nstages(L);
+    for (int s = 1; s < S; ++s) {
+        const int r = qx_radix(L, s), Ns = qx_span(L, s), stw = L / (Ns * r);
+        for (int m = 1; m < r; ++m)
+            for (int k = 0; k < Ns; ++k) out[qx_tw_index(L, Ns, m, k)] = nat[(k * m * stw) % L];
+    }
 }
 
 // rows per block for x passes: T*P ~ 256 threads, P | rows
