@@ -308,3 +308,23 @@ def test_tma_and_direct_strided_kernels_agree(dim, N, dtype):
     assert v_err(outs[1][1], outs[0][1], dtype) < tol_v
     assert outs[0][2][0] == pytest.approx(outs[1][2][0], rel=tol)
     assert outs[0][2][1] == pytest.approx(outs[1][2][1], rel=tol)
+
+
+def test_fp32_kick_accuracy():
+    """The FP32 kick psi exp(-i dt V) against FP64 on the same FP32 inputs, for
+    phases across many quadrants and for small phases."""
+    rng = np.random.default_rng(7)
+    N = 32
+    f = qx.Field(3, N, dtype="c64")
+    shape = f.shape
+    psi = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(np.complex64).astype(np.complex128)
+    for dt, vmax in ((1.0, 60.0), (1.0, 3.0), (1e-3, 0.05)):
+        V = (rng.uniform(-vmax, vmax, size=shape)).astype(np.float32).astype(np.float64)
+        f.psi = psi
+        f.V = V
+        f.kick(dt)
+        got = f.psi
+        ref = psi * np.exp(-1j * dt * V)
+        err = np.abs(got - ref) / np.abs(psi)
+        assert err.max() < 4e-7, (dt, vmax, err.max())
+    f.close()
