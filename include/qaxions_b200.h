@@ -140,6 +140,36 @@ int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbu
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 int qx_sync(qx_field_t *h);
 
+/* ---- ensemble of independent boxes (no counterpart in the reference, which
+ * runs one box per process, src/main.cxx:34-53) ----
+ * ngroups groups of boxes; group g holds boxes[g] boxes of size N[g]^dim, all
+ * with the same L, pref, dtype and dt.  The boxes of a group are stacked in one
+ * device array, so every pass of a step is one persistent launch over the
+ * tiles of all of the group's boxes; each group's loop body is replayed from a
+ * CUDA graph on its own stream and the groups run concurrently.  Boxes are
+ * numbered group by group.  Single-box operations (spectrum, Vhat, FFT plugin)
+ * are not available on ensemble boxes.  Errors: qx_ens_last_error(h). */
+typedef struct qx_ens_s qx_ens_t;
+int qx_ens_create(int ngroups, const int *N, const int *boxes, int dim, double L, double pref, int dtype,
+                  double dt, qx_ens_t **out);
+int qx_ens_destroy(qx_ens_t *h);
+const char *qx_ens_last_error(const qx_ens_t *h);
+/* number of boxes and total sites */
+int qx_ens_size(qx_ens_t *h, int *nboxes, long long *sites);
+/* grid size of one box */
+int qx_ens_box_n(qx_ens_t *h, int box, int *N);
+/* initial conditions as qx_ic_config, box b seeded with seed_base + b */
+int qx_ens_ic_config(qx_ens_t *h, int kind, unsigned long long seed_base, int n_sol, double rc_lo,
+                     double rc_hi, double sigma, double kc_factor, double clip, double rho0);
+int qx_ens_set_psi(qx_ens_t *h, int box, const double *psi);
+int qx_ens_get_psi(qx_ens_t *h, int box, double *psi);
+/* nsteps merged KDK steps of every box (returns when all are done) */
+int qx_ens_step(qx_ens_t *h, int nsteps);
+/* device time of qx_ens_step(nsteps) over all groups (events on the groups' streams) */
+int qx_ens_time_steps(qx_ens_t *h, int nsteps, float *ms);
+/* mass sum |psi|^2 dV of every box (nboxes doubles) */
+int qx_ens_mass(qx_ens_t *h, double *M);
+
 /* Allocation-free density statistics of a psi array in the CALLER's device
  * memory (no counterpart in the reference).  For callers that may not allocate
  * device memory while they run: an application whose own pool or caching

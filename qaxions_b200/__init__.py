@@ -77,6 +77,17 @@ _SIGS = {
     "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
+    "qx_ens_create": ([_i, _ip, _ip, _i, _d, _d, _i, _d, C.POINTER(_vp)], _i),
+    "qx_ens_destroy": ([_vp], _i),
+    "qx_ens_last_error": ([_vp], C.c_char_p),
+    "qx_ens_size": ([_vp, _ip, _llp], _i),
+    "qx_ens_box_n": ([_vp, _i, _ip], _i),
+    "qx_ens_ic_config": ([_vp, _i, C.c_ulonglong, _i, _d, _d, _d, _d, _d, _d], _i),
+    "qx_ens_set_psi": ([_vp, _i, _dp], _i),
+    "qx_ens_get_psi": ([_vp, _i, _dp], _i),
+    "qx_ens_step": ([_vp, _i], _i),
+    "qx_ens_time_steps": ([_vp, _i, _fp], _i),
+    "qx_ens_mass": ([_vp, _dp], _i),
 }
 for _name, (_args, _res) in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -354,3 +365,113 @@ class Field:
 
     def sync(self):
         self._c("qx_sync")
+
+
+def _ens_check(status: int, h):
+    if status != QX_OK:
+        msg = (_lib.qx_ens_last_error(h) or b"").decode(errors="replace")
+        if status == QX_ERR_INVALID:
+            raise ValueError(msg)
+        if status == QX_ERR_NOMEM:
+            raise MemoryError(msg)
+        raise QxError(status, msg)
+
+
+class Ensemble:
+    """Independent boxes of uneven sizes advanced together (no reference
+    counterpart: the reference runs one box per process, src/main.cxx:34-53).
+
+    ``groups`` is a list of (N, count): count boxes of N^dim sites each.  Boxes
+    of one size share one batched device array, so each pass of a step is one
+    persistent launch over all of their tiles; groups run concurrently, each
+    replaying its loop body from a CUDA graph.  Boxes are numbered group by
+    group; box b's initial condition is seeded with seed_base + b.
+    """
+
+    def __init__(self, groups, dim: int = 3, L: float = 1.0, pref: float = 1.0, dtype: str = "c64",
+                 dt: float | None = None):
+        ns = [int(n) for n, _ in groups]
+        cs = [int(c) for _, c in groups]
+        if dt is None:
+            dt = 0.2 / max(ns) ** 2
+        NA = (C.c_int * len(ns))(*ns)
+        CA = (C.c_int * len(cs))(*cs)
+        h = _vp()
+        st = _lib.qx_ens_create(len(ns), NA, CA, dim, L, pref, QX_C128 if dtype == "c128" else QX_C64, dt,
+                                C.byref(h))
+        _ens_check(st, None)
+        self._h = h
+        self.dim = dim
+        self.dtype = dtype
+        n = C.c_int()
+        sites = C.c_longlong()
+        _ens_check(_lib.qx_ens_size(self._h, C.byref(n), C.byref(sites)), self._h)
+        self.nboxes = n.value
+        self.sites = sites.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.qx_ens_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, name, *args):
+        _ens_check(getattr(_lib, name)(self._h, *args), self._h)
+
+    def box_n(self, box: int) -> int:
+        n = C.c_int()
+        self._c("qx_ens_box_n", box, C.byref(n))
+        return n.value
+
+    def box_shape(self, box: int):
+        return (self.box_n(box),) * self.dim
+
+    def ic_config(self, kind: int = IC_GRF, seed_base: int = 1234, n_sol: int = 0, rc_lo: float = 0.01,
+                  rc_hi: float = 0.03, sigma: float = 0.3, kc_factor: float = 0.125, clip: float = -0.9,
+                  rho0: float = 1e-6):
+        self._c("qx_ens_ic_config", kind, seed_base, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0)
+
+    def psi(self, box: int) -> np.ndarray:
+        a = np.empty(self.box_shape(box), np.complex128)
+        self._c("qx_ens_get_psi", box, _ptr(a.view(np.float64)))
+        return a
+
+    def set_psi(self, box: int, value):
+        a = np.ascontiguousarray(value, dtype=np.complex128).reshape(self.box_shape(box))
+        self._c("qx_ens_set_psi", box, _ptr(a.view(np.float64)))
+
+    def step(self, nsteps: int):
+        self._c("qx_ens_step", nsteps)
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = C.c_float()
+        self._c("qx_ens_time_steps", nsteps, C.byref(ms))
+        return ms.value
+
+    def mass(self) -> np.ndarray:
+        m = np.empty(self.nboxes, np.float64)
+        self._c("qx_ens_mass", _ptr(m))
+        return m
+
+
+def shard_groups(groups, world: int, rank: int):
+    """Instance sharding of an ensemble over `world` ranks with no collective:
+    the boxes, numbered group by group, are dealt out round-robin, so every
+    rank gets a near-equal share of every size.  Returns (groups_of_rank,
+    global box indices of rank) with groups_of_rank in the (N, count) form of
+    Ensemble (sizes with no box on this rank are left out)."""
+    boxes = []
+    for n, c in groups:
+        boxes += [int(n)] * int(c)
+    mine = [b for b in range(len(boxes)) if b % world == rank]
+    out = []
+    for n, _ in groups:
+        k = sum(1 for b in mine if boxes[b] == int(n))
+        if k:
+            out.append((int(n), k))
+    return out, mine

@@ -288,3 +288,207 @@ int qx_device_pointers(qx_field_t* h, void** psi, void** V) {
 int qx_sync(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.sync(); }); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// ensemble of independent boxes: one batched field per box size
+// ---------------------------------------------------------------------------
+
+struct qx_ens_s {
+    std::vector<std::unique_ptr<qx::Field>> groups;
+    std::vector<int> group_of;  // box -> group
+    std::vector<int> index_in;  // box -> index within its group
+    long long sites = 0;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_ens_err;
+
+template <typename F>
+int ens_guarded(qx_ens_t* h, F&& fn) {
+    if (!h) {
+        g_ens_err = "null qx_ens handle";
+        return QX_ERR_INVALID;
+    }
+    try {
+        fn(*h);
+        h->err.clear();
+        return QX_OK;
+    } catch (const std::invalid_argument& e) {
+        h->err = e.what();
+        return QX_ERR_INVALID;
+    } catch (const std::bad_alloc&) {
+        h->err = "device allocation failed";
+        return QX_ERR_NOMEM;
+    } catch (const std::logic_error& e) {
+        h->err = e.what();
+        return QX_ERR_STATE;
+    } catch (const std::runtime_error& e) {
+        h->err = e.what();
+        return QX_ERR_CUDA;
+    } catch (...) {
+        h->err = "unknown error";
+        return QX_ERR_INTERNAL;
+    }
+}
+
+void ens_box(const qx_ens_t& e, int box) {
+    need(box >= 0 && box < (int)e.group_of.size(), "box index out of range");
+}
+
+#define QX_CU(call)                                                                            \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+}  // namespace
+
+extern "C" {
+
+int qx_ens_create(int ngroups, const int* N, const int* boxes, int dim, double L, double pref, int dtype,
+                  double dt, qx_ens_t** out) {
+    if (!out) {
+        g_ens_err = "out must not be NULL";
+        return QX_ERR_INVALID;
+    }
+    *out = nullptr;
+    auto h = new qx_ens_s();
+    const int rc = ens_guarded(h, [&](qx_ens_s& e) {
+        need(ngroups > 0 && N && boxes, "need at least one group");
+        need(dtype == QX_C128 || dtype == QX_C64, "dtype must be QX_C128 or QX_C64");
+        for (int g = 0; g < ngroups; ++g) {
+            need(boxes[g] > 0, "every group needs at least one box");
+            qx::FieldConfig c;
+            c.dim = dim;
+            c.N = N[g];
+            c.L = L;
+            c.pref = pref;
+            c.rho_mean = 1.0;
+            c.prec = dtype == QX_C128 ? qx::Prec::F64 : qx::Prec::F32;
+            c.k0 = qx::K0::Zero;
+            c.dt = dt;
+            c.batch = boxes[g];
+            e.groups.push_back(qx::make_field(c));
+            for (int b = 0; b < boxes[g]; ++b) {
+                e.group_of.push_back(g);
+                e.index_in.push_back(b);
+            }
+            e.sites += (long long)e.groups.back()->sites();
+        }
+    });
+    if (rc != QX_OK) {
+        g_ens_err = h->err;
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return QX_OK;
+}
+
+int qx_ens_destroy(qx_ens_t* h) {
+    if (!h) return QX_OK;
+    try {
+        h->groups.clear();
+    } catch (...) {
+    }
+    delete h;
+    return QX_OK;
+}
+
+const char* qx_ens_last_error(const qx_ens_t* h) {
+    if (h && !h->err.empty()) return h->err.c_str();
+    return g_ens_err.c_str();
+}
+
+int qx_ens_size(qx_ens_t* h, int* nboxes, long long* sites) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        if (nboxes) *nboxes = (int)e.group_of.size();
+        if (sites) *sites = e.sites;
+    });
+}
+
+int qx_ens_box_n(qx_ens_t* h, int box, int* N) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        ens_box(e, box);
+        need(N != nullptr, "N must not be NULL");
+        *N = e.groups[e.group_of[box]]->size();
+    });
+}
+
+int qx_ens_ic_config(qx_ens_t* h, int kind, unsigned long long seed_base, int n_sol, double rc_lo, double rc_hi,
+                     double sigma, double kc_factor, double clip, double rho0) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(kind == QX_IC_GRF || kind == QX_IC_SOLITONS, "kind must be QX_IC_GRF or QX_IC_SOLITONS");
+        need(n_sol >= 0, "n_sol must be >= 0");
+        for (size_t i = 0; i < e.group_of.size(); ++i)
+            e.groups[e.group_of[i]]->ic_config_box(e.index_in[i], kind, seed_base + i, n_sol, rc_lo, rc_hi, sigma,
+                                                   kc_factor, clip, rho0);
+    });
+}
+
+int qx_ens_set_psi(qx_ens_t* h, int box, const double* psi) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        ens_box(e, box);
+        need(psi != nullptr, "psi must not be NULL");
+        e.groups[e.group_of[box]]->set_psi_box(e.index_in[box], psi);
+    });
+}
+
+int qx_ens_get_psi(qx_ens_t* h, int box, double* psi) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        ens_box(e, box);
+        need(psi != nullptr, "psi must not be NULL");
+        e.groups[e.group_of[box]]->get_psi_box(e.index_in[box], psi);
+    });
+}
+
+int qx_ens_step(qx_ens_t* h, int nsteps) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(nsteps >= 0, "nsteps must be >= 0");
+        for (auto& g : e.groups) g->step(nsteps);  // enqueued on each group's stream
+        for (auto& g : e.groups) g->sync();
+    });
+}
+
+int qx_ens_time_steps(qx_ens_t* h, int nsteps, float* ms) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(nsteps > 0 && ms, "nsteps must be > 0 and ms not NULL");
+        // first group's stream brackets the others: start event -> all wait,
+        // every group's end event -> first stream waits -> stop event
+        cudaStream_t s0 = e.groups[0]->stream();
+        cudaEvent_t start, stop;
+        std::vector<cudaEvent_t> ends(e.groups.size());
+        QX_CU(cudaEventCreate(&start));
+        QX_CU(cudaEventCreate(&stop));
+        for (auto& ev : ends) QX_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        QX_CU(cudaEventRecord(start, s0));
+        for (auto& g : e.groups) QX_CU(cudaStreamWaitEvent(g->stream(), start, 0));
+        for (size_t i = 0; i < e.groups.size(); ++i) {
+            e.groups[i]->step(nsteps);
+            QX_CU(cudaEventRecord(ends[i], e.groups[i]->stream()));
+        }
+        for (auto& ev : ends) QX_CU(cudaStreamWaitEvent(s0, ev, 0));
+        QX_CU(cudaEventRecord(stop, s0));
+        QX_CU(cudaEventSynchronize(stop));
+        float t = 0.f;
+        QX_CU(cudaEventElapsedTime(&t, start, stop));
+        for (auto& g : e.groups) g->sync();
+        for (auto& ev : ends) cudaEventDestroy(ev);
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        *ms = t;
+    });
+}
+
+int qx_ens_mass(qx_ens_t* h, double* M) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(M != nullptr, "M must not be NULL");
+        size_t off = 0;
+        for (auto& g : e.groups) {
+            g->box_mass(M + off);
+            off += (size_t)g->batch();
+        }
+    });
+}
+
+}  // extern "C"

@@ -224,6 +224,7 @@ static typename Ops<R>::SP sp0(int* err, const Geometry& g, typename Ops<R>::C* 
     s.X = X;
     s.dim = g.dim;
     s.N = g.N;
+    s.batch = g.B;
     s.scale = 1.0;
     return s;
 }
@@ -234,7 +235,7 @@ template <typename R> void B200FFTBackend<R>::forward_c2c(void* data) {
     a.in = d;
     a.out = d;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, tw_, g_.N), -1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,d, tw_, g_.N), -1, *tune_, st_);
     Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, tw_, g_.N), OP_FWD, *tune_, st_);
 }
 
@@ -243,13 +244,13 @@ template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C
     a.in = in;
     a.out = out;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,out, tw_, g_.N), -1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,out, tw_, g_.N), -1, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2c(void* data) {
     C* d = static_cast<C*>(data);
     Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, tw_, g_.N), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,d, tw_, g_.N), +1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,d, tw_, g_.N), +1, *tune_, st_);
     auto a = xp0<R>(g_, tw_);
     a.in = d;
     a.out = d;
@@ -262,14 +263,14 @@ template <typename R> void B200FFTBackend<R>::forward_r2c(void* in_real, void* o
     a.Vin = static_cast<const R*>(in_real);
     a.vh = h;
     Ops<R>::x_r2c(g_.N, a, true, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), -1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), -1, *tune_, st_);
     Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2r(void* in_half, void* out_real) {
     C* h = static_cast<C*>(in_half);
     Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), +1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), +1, *tune_, st_);
     auto a = xp0<R>(g_, tw_);
     a.vh = h;
     a.Vout = static_cast<R*>(out_real);
@@ -316,8 +317,11 @@ class FieldT final : public Field {
         QX_CUDA(cudaGetDevice(&device_));
         g_.dim = cfg.dim;
         g_.N = cfg.N;
-        g_.rows = cfg.dim == 3 ? (long)cfg.N * cfg.N : cfg.N;
+        if (cfg.batch < 1) throw std::invalid_argument("batch must be >= 1");
+        g_.B = cfg.batch;
+        g_.rows = (long)cfg.batch * (cfg.dim == 3 ? (long)cfg.N * cfg.N : cfg.N);
         g_.S = g_.rows * cfg.N;
+        g_.S1 = g_.S / cfg.batch;
         g_.hsites = g_.rows * (cfg.N / 2);
         ds_ = cfg.dt;
         QX_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
@@ -365,8 +369,9 @@ class FieldT final : public Field {
 
     // ---- derived constants ----
     double dk() const { return kTwoPi / cfg_.L; }
-    double pois_c() const { return -1.0 / (dk() * dk() * (double)g_.S); }
-    double pois_g0() const { return cfg_.k0 == K0::Reference ? -1.0 / (double)g_.S : 0.0; }
+    // FFT normalisations are per box (S1 sites; S1 = S for a single box)
+    double pois_c() const { return -1.0 / (dk() * dk() * (double)g_.S1); }
+    double pois_g0() const { return cfg_.k0 == K0::Reference ? -1.0 / (double)g_.S1 : 0.0; }
     C* psi() { return psi_.as<C>(); }
     R* V() { return V_.as<R>(); }
     C* vh() { return vh_.as<C>(); }
@@ -376,15 +381,15 @@ class FieldT final : public Field {
 
     // ---- pass sequences ----
     void y_fwd(C* a, int X) {
-        if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp(a, X), -1, tune_, st_);
+        if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp(a, X), -1, tune_, st_);
     }
     void y_inv(C* a, int X) {
-        if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.N, sp(a, X), +1, tune_, st_);
+        if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp(a, X), +1, tune_, st_);
     }
     void la_drift(double dt) {
         auto s = sp(psi(), g_.N);
         s.phase_fac = -0.5 * dt * dk() * dk();
-        s.scale = 1.0 / (double)g_.S;
+        s.scale = 1.0 / (double)g_.S1;
         Ops<R>::la_pass(g_.N, s, OP_DRIFT, tune_, st_);
     }
     void la_poisson() {
@@ -420,7 +425,10 @@ class FieldT final : public Field {
         v_current_ = false;
     }
 
-    void Poisson() override { Misc<R>::poisson_packed(vh(), g_.dim, g_.N, pois_c(), pois_g0(), st_); }
+    void Poisson() override {
+        single_box("Poisson");
+        Misc<R>::poisson_packed(vh(), g_.dim, g_.N, pois_c(), pois_g0(), st_);
+    }
 
     void updatePotential() override {  // src/field.cxx:294-346
         density_r2c_partial();
@@ -564,7 +572,7 @@ class FieldT final : public Field {
         double ks = 0.0;
         QX_CUDA(cudaMemcpyAsync(&ks, redout_.p, sizeof(double), cudaMemcpyDeviceToHost, st_));
         QX_CUDA(cudaStreamSynchronize(st_));
-        const double kin = 0.5 * dV / (double)g_.S * dk() * dk() * ks;
+        const double kin = 0.5 * dV / (double)g_.S1 * dk() * dk() * ks;
         if (M) *M = m;
         if (K) *K = kin;
         if (W) *W = w;
@@ -572,6 +580,7 @@ class FieldT final : public Field {
     }
 
     void spectrum(int source, int mode, int nbins, double* k, double* P, long long* count) override {
+        single_box("spectrum");
         if (mode < 0 || mode > 2) throw std::invalid_argument("spectrum mode must be 0, 1 or 2");
         if (mode == 0) nbins = g_.N / 2 + 1;
         if (nbins <= 0 || nbins > 4096) throw std::invalid_argument("nbins out of range");
@@ -626,16 +635,16 @@ class FieldT final : public Field {
     // ---- host buffers ----
     void stage_alloc(size_t bytes) { stage_.alloc(bytes); }
 
-    void set_psi(const double* h) override {
+    void upload_psi(const double* h, C* dst, long n_el) {
         if constexpr (sizeof(R) == 8) {
-            QX_CUDA(cudaMemcpyAsync(psi_.p, h, sizeof(C) * g_.S, cudaMemcpyHostToDevice, st_));
+            QX_CUDA(cudaMemcpyAsync(dst, h, sizeof(C) * n_el, cudaMemcpyHostToDevice, st_));
         } else {
             const long chunk = 1L << 22;
             stage_alloc(sizeof(double2) * chunk);
-            for (long o = 0; o < g_.S; o += chunk) {
-                const long n = std::min(chunk, g_.S - o);
+            for (long o = 0; o < n_el; o += chunk) {
+                const long n = std::min(chunk, n_el - o);
                 QX_CUDA(cudaMemcpyAsync(stage_.p, h + 2 * o, sizeof(double2) * n, cudaMemcpyHostToDevice, st_));
-                Misc<R>::from_f64(stage_.as<double2>(), psi() + o, n, st_);
+                Misc<R>::from_f64(stage_.as<double2>(), dst + o, n, st_);
             }
         }
         QX_CUDA(cudaStreamSynchronize(st_));
@@ -643,7 +652,56 @@ class FieldT final : public Field {
         vmax_stale_ = true;
     }
 
+    void set_psi(const double* h) override { upload_psi(h, psi(), g_.S); }
+
     void get_psi(double* h) override { download_c(psi(), g_.S, h); }
+
+    // ---- boxes of a batched field ----
+    void check_box(int box) const {
+        if (box < 0 || box >= g_.B) throw std::invalid_argument("box index out of range");
+    }
+    void single_box(const char* what) const {
+        if (g_.B != 1) throw std::invalid_argument(std::string(what) + " needs a single-box field (batch 1)");
+    }
+    void set_psi_box(int box, const double* h) override {
+        check_box(box);
+        upload_psi(h, psi() + (long)box * g_.S1, g_.S1);
+    }
+    void get_psi_box(int box, double* h) override {
+        check_box(box);
+        download_c(psi() + (long)box * g_.S1, g_.S1, h);
+    }
+    void box_mass(double* M) override {
+        const double dV = std::pow(cfg_.L / g_.N, g_.dim);
+        std::vector<double> h(2 * g_.B);
+        for (int b = 0; b < g_.B; ++b) {
+            Misc<R>::reduce(RED_RHO, psi() + (long)b * g_.S1, V() + (long)b * g_.S1, g_.S1, red_.as<double>(),
+                            redout_.as<double>(), st_);
+            QX_CUDA(cudaMemcpyAsync(&h[2 * b], redout_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
+            QX_CUDA(cudaStreamSynchronize(st_));
+        }
+        for (int b = 0; b < g_.B; ++b) M[b] = h[2 * b] * dV;
+    }
+    void ic_config_box(int box, int kind, uint64_t seed, int n_sol, double rc_lo, double rc_hi, double sigma,
+                       double kc_factor, double clip, double rho0) override {
+        check_box(box);
+        FieldConfig c = cfg_;
+        c.prec = Prec::F64;
+        c.batch = 1;
+        FieldT<double> tmp(c);
+        tmp.ic_config(kind, seed, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0);
+        QX_CUDA(cudaStreamSynchronize(tmp.stream()));
+        const double2* src = reinterpret_cast<const double2*>(tmp.psi_device());
+        C* dst = psi() + (long)box * g_.S1;
+        if constexpr (sizeof(R) == 8) {
+            QX_CUDA(cudaMemcpyAsync(dst, src, sizeof(C) * g_.S1, cudaMemcpyDeviceToDevice, st_));
+        } else {
+            Misc<R>::from_f64(src, dst, g_.S1, st_);
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+        v_current_ = false;
+        vmax_stale_ = true;
+    }
 
     void download_c(const C* d, long n_el, double* h) {
         if constexpr (sizeof(R) == 8) {
@@ -712,11 +770,13 @@ class FieldT final : public Field {
     void get_V(double* h) override { download_r(V(), g_.S, h); }
 
     void get_Vhat(double* h) override {
+        single_box("get_Vhat");
         std::vector<double> packed(2 * g_.hsites);
         download_c(vh(), g_.hsites, packed.data());
         unpack_half(g_.dim, g_.N, packed.data(), h);
     }
     void set_Vhat(const double* h) override {
+        single_box("set_Vhat");
         std::vector<double> packed(2 * g_.hsites);
         pack_half(g_.dim, g_.N, h, packed.data());
         upload_c(packed.data(), vh(), g_.hsites);
@@ -724,6 +784,7 @@ class FieldT final : public Field {
 
     // ---- FFT plugin on host buffers (uses the measurement scratch) ----
     void host_c2c(double* data, int sign) override {
+        single_box("host_c2c");
         mpsi_.alloc(sizeof(C) * g_.S);
         upload_c(data, mpsi_.as<C>(), g_.S);
         if (sign < 0) fft_->forward_c2c(mpsi_.p);
@@ -731,6 +792,7 @@ class FieldT final : public Field {
         download_c(mpsi_.as<C>(), g_.S, data);
     }
     void host_r2c(const double* in, double* out) override {
+        single_box("host_r2c");
         mpsi_.alloc(sizeof(C) * g_.S);  // real staging inside the complex scratch
         mvh_.alloc(sizeof(C) * g_.hsites);
         upload_r(in, reinterpret_cast<R*>(mpsi_.p), g_.S);
@@ -740,6 +802,7 @@ class FieldT final : public Field {
         unpack_half(g_.dim, g_.N, packed.data(), out);
     }
     void host_c2r(const double* in, double* out) override {
+        single_box("host_c2r");
         mpsi_.alloc(sizeof(C) * g_.S);
         mvh_.alloc(sizeof(C) * g_.hsites);
         std::vector<double> packed(2 * g_.hsites);
@@ -752,6 +815,7 @@ class FieldT final : public Field {
 
     // ---- initial conditions ----
     void ic_gaussian_solitons(int n, const double* rows5, double bkg) override {
+        single_box("ic_gaussian_solitons");
         if constexpr (sizeof(R) == 8) {
             DevBuf rows;
             rows.alloc(sizeof(double) * 5 * (n > 0 ? n : 1));
@@ -773,6 +837,11 @@ class FieldT final : public Field {
 
     void ic_config(int kind, uint64_t seed, int n_sol, double rc_lo, double rc_hi, double sigma,
                    double kc_factor, double clip, double rho0) override {
+        if (g_.B > 1) {  // an ensemble group: box b gets seed + b
+            for (int b = 0; b < g_.B; ++b)
+                ic_config_box(b, kind, seed + (uint64_t)b, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0);
+            return;
+        }
         if constexpr (sizeof(R) == 8) {
             double2* p = reinterpret_cast<double2*>(psi());
             if (kind == 0) {

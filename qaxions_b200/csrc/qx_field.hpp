@@ -38,6 +38,7 @@ struct FieldConfig {
     K0 k0 = K0::Reference;
     double dt = 1e-4;       // ds_ used by half_kick/full_kick/drift_update/step
     int device = -1;        // CUDA device (-1: current)
+    int batch = 1;          // boxes of this size stacked in one array (an ensemble group)
 };
 
 // Device-side FFT plugin: in-place c2c, r2c into the packed half spectrum,
@@ -58,9 +59,12 @@ class FFTBackend {
     virtual ptrdiff_t global_N() const = 0;
 };
 
+// S, rows and hsites count every box of a batched field; S1 is one box
 struct Geometry {
     int dim, N;
     long S, rows, hsites;
+    int B = 1;
+    long S1 = 0;
     long fftw_ksites() const { return rows * (N / 2 + 1); }
 };
 
@@ -144,6 +148,14 @@ class Field {
     virtual void ic_gaussian_solitons(int n, const double* rows5, double bkg) = 0;
     virtual void ic_config(int kind, uint64_t seed, int n_sol, double rc_lo, double rc_hi, double sigma,
                            double kc_factor, double clip, double rho0) = 0;
+
+    // ---- boxes of a batched field (batch > 1: an ensemble group) ----
+    int batch() const { return g_.B; }
+    virtual void ic_config_box(int box, int kind, uint64_t seed, int n_sol, double rc_lo, double rc_hi,
+                               double sigma, double kc_factor, double clip, double rho0) = 0;
+    virtual void set_psi_box(int box, const double* interleaved) = 0;
+    virtual void get_psi_box(int box, double* interleaved) = 0;
+    virtual void box_mass(double* M) = 0;  // per-box sum |psi|^2 dV
 
     // ---- timing / device access ----
     virtual float time_steps(int nsteps, int use_graph) = 0;  // device ms of step(nsteps)

@@ -34,6 +34,7 @@ template <typename R> struct Ops {
     };
     struct SP {
         C* a; const C* tw; const C* tw_lo; int X, dim, N;
+        int batch;  // boxes stacked in the array (0 or 1: a single box)
         double phase_fac, scale, pois_c, pois_g0; double* partial;
         int* err;  // device flag set when a bounded wait times out
     };

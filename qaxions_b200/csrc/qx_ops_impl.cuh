@@ -428,7 +428,8 @@ static void launch_col0(const typename Ops<R>::SP& a, cudaStream_t st) {
     using C = cx_t<R>;
     constexpr int E0 = qx_lcm_radices(NN);
     dim3 blk(2, NN / E0, 1);
-    k_poisson_col0<NN, R><<<NN / 2, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.tw_lo, a.pois_c, a.pois_g0);
+    dim3 grd(NN / 2, a.batch > 0 ? a.batch : 1);
+    k_poisson_col0<NN, R><<<grd, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.tw_lo, a.pois_c, a.pois_g0);
     QX_LAUNCH_CHECK();
 }
 
@@ -440,7 +441,8 @@ long Ops<R>::la_pass(int N, const SP& a, int op, const Tune& tu, cudaStream_t st
     if (tu.tma) {
         QX_FOR_N(N, {
             const int d3 = a.dim == 3 ? 1 : 0;
-            const int NZ = d3 ? NN : 1, outer = d3 ? NN : 1, pdim = d3 ? 2 : 1;
+            const int nb = a.batch > 0 ? a.batch : 1;
+            const int NZ = d3 ? nb * NN : nb, outer = d3 ? nb * NN : nb, pdim = d3 ? 2 : 1;
             long grid = 0;
             switch (op) {
                 case OP_FWD: grid = launch_tma<NN, R, OP_FWD>(a, NZ, outer, pdim, d3, 0, tu, st); break;
@@ -456,6 +458,7 @@ long Ops<R>::la_pass(int N, const SP& a, int op, const Tune& tu, cudaStream_t st
             return grid;
         });
     }
+    if (a.batch > 1) throw std::invalid_argument("batched arrays need the TMA-fed strided passes");
     QX_FOR_N(N, {
         constexpr int E = qx_col_e(NN);
         const int T = NN / E;

@@ -139,7 +139,8 @@ template <typename R> struct TArgs {
     const cx_t<R>* tw_lo;  // exact - tw (FP32 double-float twiddles), global
     int X;               // columns (N for psi, N/2 for the packed half spectrum)
     int N;
-    int outer;           // tiles along the non-pencil axis (z for y passes, y for z passes, 1 in 2D)
+    int outer;           // tiles along the non-pencil axis (z planes for y passes, box * N + y for
+                         // 3D z passes, boxes in 2D; batched arrays stack boxes along z)
     int pencil_dim;      // 1: pencil along tensor dim 1 (y passes, 2D last axis); 2: along dim 2 (3D z)
     int la3d;            // last-axis pass of a 3D array (pencil = z, outer = y)
     int TX, tiles_x, nbuf, nbox, box;
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         const int o = (int)(id / s.tiles_x);
         c0 = 2 * x0;
         if (s.pencil_dim == 1) { c1 = j * s.box; c2 = o; }
-        else { c1 = o; c2 = j * s.box; }
+        else { c1 = o % N; c2 = (o / N) * N + j * s.box; }  // o = box * N + y
     };
     auto issue_load = [&](long id, int b) {
         const uint32_t bar = smem_u32(&mbar[b]);
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         auto mxy_of = [&](int h) {
             const int x = xb + h;
             const int nx = (s.X == N) ? signed_mode(x, N) : x;
-            const int ny = s.la3d ? signed_mode(o, N) : 0;
+            const int ny = s.la3d ? signed_mode(o % N, N) : 0;
             return (long)nx * nx + (long)ny * ny;
         };
         bool store = true;
@@ -389,7 +390,8 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
 // 3D Poisson, column 0: rows y and N-y (0 pairs with N/2) of the packed
 // kx = {0, N/2} column, already transformed along x, y and z, get
 // C'(k) = a C(k) + b conj C(-k) with a, b from the kx = 0 and kx = N/2
-// multipliers, then the inverse z transform.  blockDim = (2, N/E).
+// multipliers, then the inverse z transform.  blockDim = (2, N/E); grid
+// (N/2, boxes of a batched array).
 template <int N, typename R>
 __global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, const cx_t<R>* tw_lo, double pois_c,
                                double pois_g0) {
@@ -400,6 +402,7 @@ __global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, const cx_t<R>* tw
     C* sm = reinterpret_cast<C*>(smem_raw);
     const int g = threadIdx.x, t = threadIdx.y;
     const int gi = blockIdx.x;
+    vh += (long)blockIdx.y * N * N * X;  // box of a batched array
     const int ya = gi == 0 ? 0 : gi, yb = gi == 0 ? N / 2 : N - gi;
     const int y = g == 0 ? ya : yb;
     const int gm = (gi == 0) ? g : 1 - g;
