@@ -325,6 +325,85 @@ def run_ensemble(args, world, rank, local):
             "accuracy": acc}), flush=True)
 
 
+def run_corrector(args, world, rank, local):
+    """Learned-corrector workload (3D 256^3 GRF + 16 solitons, complex64):
+    the network is trained on pairs from 16 seeds at 128^3 (same dt / dx^2),
+    then one coarse step at 4 dt + correction is compared with four fused fine
+    steps and with the coarse step alone: errors against a plain FP64 fine run
+    after the same simulated time, and simulated time per wall-second."""
+    if rank != 0:
+        return
+    import time as _t
+
+    import qaxions_b200 as qx
+    from qaxions_b200 import corrector as cr
+    qx.set_device(local)
+    N, NT = 256, 128
+    dt, dtt = 0.2 / N**2, 0.2 / NT**2
+    ncoarse = max(args.steps, 4)
+    corr_t = cr.Corrector(NT, seed=1)
+    t0 = _t.time()
+    losses = cr.train(corr_t, seeds=list(range(1, 17)), pairs_per_seed=args.corr_pairs, dt=dtt, lr=2e-3, n_sol=16)
+    t_train = _t.time() - t0
+    corr = cr.Corrector(N, seed=0)
+    corr.params = corr_t.params
+    corr.set_scales(*corr_t.scales())
+    corr_t.close()
+
+    def field(dtype, d):
+        f = qx.Field(3, N, dtype=dtype, k0="zero", dt=d)
+        f.ic_config(qx.IC_GRF, 1234, 16, 0.01, 0.03)
+        return f
+
+    ref = field("c128", dt)
+    ref.step(4 * ncoarse)
+    pref_ = ref.psi
+    M0 = 1.0
+    fine = field("c64", dt)
+    fine.step(4 * ncoarse)
+    coarse = field("c64", 4 * dt)
+    coarse.step(ncoarse)
+    corrd = field("c64", dt)
+    fb = cr.corrected_steps(corrd, corr, ncoarse, dt, tol=1e-6)
+    errs = {k: float(np.linalg.norm(f.psi - pref_) / np.linalg.norm(pref_)) for k, f in
+            (("fine_fp32", fine), ("coarse_fp32", coarse), ("corrected_fp32", corrd))}
+    mass = {k: abs(f.mass_energy()[0] - M0) for k, f in
+            (("fine_fp32", fine), ("coarse_fp32", coarse), ("corrected_fp32", corrd))}
+    # timing (device events for the plain forms; wall clock around the corrected loop)
+    ms_fine = fine.time_steps(20, True) / 20
+    coarse.set_dt(4 * dt)
+    ms_coarse = coarse.time_steps(20, True) / 20
+    corrd.sync()
+    t0 = _t.time()
+    for _ in range(5):
+        corrd.set_dt(4 * dt)
+        corrd.step(1)
+        corr.apply(corrd)
+    corrd.sync()
+    ms_net_step = (_t.time() - t0) / 5 * 1e3
+    t0 = _t.time()
+    cr.corrected_steps(corrd, corr, 3, dt, tol=np.inf)
+    ms_checked = (_t.time() - t0) / 3 * 1e3
+    sim = {"fine_fp32": dt / (ms_fine * 1e-3), "coarse_fp32": 4 * dt / (ms_coarse * 1e-3),
+           "corrected_fp32": 4 * dt / (ms_net_step * 1e-3),
+           "corrected_fp32_with_checks": 4 * dt / (ms_checked * 1e-3)}
+    print(json.dumps({
+        "metric": "simulated time per wall-second, learned-corrector form vs fused form (256^3)",
+        "value": sim["corrected_fp32"] / sim["fine_fp32"], "unit": "x fused form",
+        "n_gpus": 1, "steps": ncoarse, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 + bf16 network", "data": "synthetic",
+        "config": {"workload": "3D 256^3 GRF + 16 Schive solitons, dt = 0.2 dx^2, coarse 4 dt",
+                   "train": f"128^3, 16 seeds x {args.corr_pairs} pairs, Adam 2e-3, {t_train:.1f} s",
+                   "loss_first": losses[0], "loss_last10": float(np.mean(losses[-10:]))},
+        "errors_vs_fp64_fine": errs, "mass_drift": mass, "fallbacks": fb, "coarse_steps": ncoarse,
+        "ms": {"fused_fine_step": ms_fine, "coarse_step": ms_coarse, "coarse_step_plus_network": ms_net_step,
+               "corrected_step_with_mass_energy_checks": ms_checked},
+        "sim_time_per_wall_s": sim}), flush=True)
+    for f in (ref, fine, coarse, corrd):
+        f.close()
+    corr.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,11 +412,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--accuracy-steps", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="kdk512", choices=["kdk512", "ensemble"],
-                    help="kdk512: the 512^3 single-box step (default); ensemble: 16x64^3 + 16x96^3 + 16x128^3 boxes")
+    ap.add_argument("--workload", default="kdk512", choices=["kdk512", "ensemble", "corrector"],
+                    help="kdk512: the 512^3 single-box step (default); ensemble: 16x64^3 + 16x96^3 + 16x128^3 "
+                         "boxes; corrector: learned-corrector form at 256^3")
+    ap.add_argument("--corr-pairs", type=int, default=8, help="training pairs per seed (corrector workload)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
+    if args.workload == "corrector" and args.impl == "ours":
+        run_corrector(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "ensemble" and args.impl == "ours":
         run_ensemble(args, world, rank, local)
         if world > 1:

@@ -138,6 +138,12 @@ int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, dou
  * passes (1 or 2; 0 = default: 2 in the FP32 form, FP64 always 1) */
 int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw);
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
+/* dst psi <- src psi on the device (same dim, N, batch and dtype) */
+int qx_copy_psi(qx_field_t *dst, qx_field_t *src);
+/* psi was written through qx_device_pointers: recompute V before it is used */
+int qx_psi_changed(qx_field_t *h);
+/* psi *= factor (real) */
+int qx_scale_psi(qx_field_t *h, double factor);
 int qx_sync(qx_field_t *h);
 
 /* ---- ensemble of independent boxes (no counterpart in the reference, which
@@ -169,6 +175,38 @@ int qx_ens_step(qx_ens_t *h, int nsteps);
 int qx_ens_time_steps(qx_ens_t *h, int nsteps, float *ms);
 /* mass sum |psi|^2 dV of every box (nboxes doubles) */
 int qx_ens_mass(qx_ens_t *h, double *M);
+
+/* ---- learned corrector for coarse steps (no counterpart in the reference) ----
+ * A periodic 3^3 convolutional network (4 -> 32 -> 32 -> 2 channels, GELU,
+ * BF16 weights on the tensor cores, FP32 accumulation) on N^3 grids (N a
+ * multiple of 8) predicts psi(4 fine steps) - psi(1 coarse step of 4 dt) from
+ * the coarse result: features Re psi, Im psi, V / v_scale, |psi|^2 - 1; output
+ * scaled by tau.  State arguments are device pointers to complex64 psi and
+ * float32 V of an N^3 field (qx_device_pointers of a QX_C64 field).
+ * Parameters (qx_corr_get/set_params, FP32): w1 [27][4][32], b1 [32],
+ * w2 [27][32][32], b2 [32], w3 [27][32][2], b3 [2]; offset index
+ * o = (dz+1)*9 + (dy+1)*3 + (dx+1).  Errors: qx_corr_last_error(h). */
+typedef struct qx_corr_s qx_corr_t;
+int qx_corr_create(int N, unsigned long long seed, qx_corr_t **out);
+int qx_corr_destroy(qx_corr_t *h);
+const char *qx_corr_last_error(const qx_corr_t *h);
+int qx_corr_nparams(qx_corr_t *h, int *n);
+int qx_corr_set_scales(qx_corr_t *h, double v_scale, double tau);
+int qx_corr_get_scales(qx_corr_t *h, double *v_scale, double *tau);
+int qx_corr_get_params(qx_corr_t *h, float *params);
+int qx_corr_set_params(qx_corr_t *h, const float *params);
+/* loss (mean square of net - (psi_f - psi_c)/tau) and its gradient (nparams
+ * floats, layout of the parameters) for one pair, without updating */
+int qx_corr_gradients(qx_corr_t *h, const void *psi_c, const void *V_c, const void *psi_f, float *grads,
+                      double *loss);
+/* one Adam step (learning rate lr) on one pair; returns the loss before it */
+int qx_corr_train_pair(qx_corr_t *h, const void *psi_c, const void *V_c, const void *psi_f, double lr,
+                       double *loss);
+/* psi += tau * net(psi, V), ordered after prior work on `stream` (a
+ * cudaStream_t, e.g. the field's) and before later work on it */
+int qx_corr_apply(qx_corr_t *h, void *psi, const void *V, void *stream);
+/* the last forward's raw output [N^3][2] (host copy) */
+int qx_corr_output(qx_corr_t *h, float *out);
 
 /* Allocation-free density statistics of a psi array in the CALLER's device
  * memory (no counterpart in the reference).  For callers that may not allocate

@@ -2,6 +2,7 @@
 // Exceptions are caught here and turned into status codes + messages.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <fstream>
 #include <new>
@@ -286,6 +287,37 @@ int qx_device_pointers(qx_field_t* h, void** psi, void** V) {
 }
 
 int qx_sync(qx_field_t* h) { return guarded(h, [&](qx::Field& f) { f.sync(); }); }
+
+}  // extern "C"
+
+extern "C" {
+
+int qx_copy_psi(qx_field_t* dst, qx_field_t* src) {
+    return guarded(dst, [&](qx::Field& d) {
+        need(src && src->f, "null source handle");
+        qx::Field& s = *src->f;
+        need(d.dim() == s.dim() && d.size() == s.size() && d.sites() == s.sites() &&
+                 d.config().prec == s.config().prec,
+             "fields differ in geometry or dtype");
+        const size_t bytes = d.sites() * (d.config().prec == qx::Prec::F64 ? 16 : 8);
+        s.sync();
+        cudaError_t e = cudaMemcpyAsync(d.psi_device(), s.psi_device(), bytes, cudaMemcpyDeviceToDevice, d.stream());
+        if (e == cudaSuccess) e = cudaStreamSynchronize(d.stream());
+        if (e != cudaSuccess) throw std::runtime_error(std::string("psi copy: ") + cudaGetErrorString(e));
+        d.psi_changed();
+    });
+}
+
+int qx_psi_changed(qx_field_t* h) {
+    return guarded(h, [&](qx::Field& f) { f.psi_changed(); });
+}
+
+int qx_scale_psi(qx_field_t* h, double factor) {
+    return guarded(h, [&](qx::Field& f) {
+        need(std::isfinite(factor), "factor must be finite");
+        f.scale_psi(factor);
+    });
+}
 
 }  // extern "C"
 

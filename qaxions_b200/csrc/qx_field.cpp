@@ -654,6 +654,17 @@ class FieldT final : public Field {
 
     void set_psi(const double* h) override { upload_psi(h, psi(), g_.S); }
 
+    void psi_changed() override {
+        v_current_ = false;
+        vmax_stale_ = true;
+    }
+
+    void scale_psi(double factor) override {
+        Misc<R>::scale(psi(), factor, g_.S, st_);
+        QX_CUDA(cudaStreamSynchronize(st_));
+        psi_changed();
+    }
+
     void get_psi(double* h) override { download_c(psi(), g_.S, h); }
 
     // ---- boxes of a batched field ----

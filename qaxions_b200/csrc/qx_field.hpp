@@ -161,6 +161,9 @@ class Field {
     virtual float time_steps(int nsteps, int use_graph) = 0;  // device ms of step(nsteps)
     virtual void profile_step(int nsteps, std::vector<std::pair<std::string, double>>& per_kernel_ms) = 0;
     virtual void* psi_device() = 0;
+    // psi was changed in place through psi_device(): drop derived state (V)
+    virtual void psi_changed() = 0;
+    virtual void scale_psi(double factor) = 0;
     virtual void* V_device() = 0;
     virtual void sync() = 0;
     cudaStream_t stream() const { return st_; }
