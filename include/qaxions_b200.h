@@ -137,6 +137,12 @@ int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, dou
  * 0 = direct loads; -1 = keep), TMA ring depth, pencils per thread of the TMA
  * passes (1 or 2; 0 = default: 2 in the FP32 form, FP64 always 1) */
 int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw);
+/* Autotuner: time nsteps steps under each candidate launch geometry (pencils
+ * per thread, TMA ring depth, tile widths, rows per x block), keep the fastest;
+ * psi is restored afterwards.  Cached per (dim, N, dtype, batch) in the process
+ * and in the text file cache_path if not NULL (read first, appended after).
+ * best_ms: ms per step of the choice; from_cache: 1 if nothing was timed. */
+int qx_autotune(qx_field_t *h, int nsteps, const char *cache_path, double *best_ms, int *from_cache);
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 /* dst psi <- src psi on the device (same dim, N, batch and dtype) */
 int qx_copy_psi(qx_field_t *dst, qx_field_t *src);

@@ -77,6 +77,7 @@ _SIGS = {
     "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
+    "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
     "qx_ens_create": ([_i, _ip, _ip, _i, _d, _d, _i, _d, C.POINTER(_vp)], _i),
     "qx_ens_destroy": ([_vp], _i),
     "qx_ens_last_error": ([_vp], C.c_char_p),
@@ -357,6 +358,15 @@ class Field:
         persistent or the direct-load strided kernels (-1 keeps the current);
         pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
         self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
+
+    def autotune(self, nsteps: int = 3, cache: str | None = None):
+        """Pick the fastest launch geometry for this grid (psi is left as it
+        was).  Returns (ms per step of the choice, whether it came from the
+        cache); `cache` names a text file shared between runs."""
+        ms = C.c_double()
+        fc = C.c_int()
+        self._c("qx_autotune", nsteps, cache.encode() if cache else None, C.byref(ms), C.byref(fc))
+        return ms.value, bool(fc.value)
 
     def device_pointers(self):
         p, v = _vp(), _vp()

@@ -308,6 +308,15 @@ int qx_copy_psi(qx_field_t* dst, qx_field_t* src) {
     });
 }
 
+int qx_autotune(qx_field_t* h, int nsteps, const char* cache_path, double* best_ms, int* from_cache) {
+    return guarded(h, [&](qx::Field& f) {
+        bool fc = false;
+        const double ms = f.autotune(nsteps, cache_path, &fc);
+        if (best_ms) *best_ms = ms;
+        if (from_cache) *from_cache = fc ? 1 : 0;
+    });
+}
+
 int qx_psi_changed(qx_field_t* h) {
     return guarded(h, [&](qx::Field& f) { f.psi_changed(); });
 }

@@ -3,6 +3,9 @@
 
 #include <cmath>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 
@@ -301,6 +304,46 @@ void Field::propagate() {  // src/field.cxx:388-402
     updateTime();
     updatePotential();
     kick(0.5 * ds_);
+}
+
+// ---------------------------------------------------------------------------
+// autotuner cache: "dim N dtype batch : x_rows y_tx la_tx tma nbuf pw ms"
+// ---------------------------------------------------------------------------
+
+static std::map<std::string, std::pair<Tune, double>>& tune_cache() {
+    static std::map<std::string, std::pair<Tune, double>> c;
+    return c;
+}
+
+static bool tune_lookup(const std::string& key, const char* path, Tune& t, double& ms) {
+    auto& c = tune_cache();
+    auto it = c.find(key);
+    if (it == c.end() && path && *path) {
+        std::ifstream in(path);
+        std::string line;
+        while (std::getline(in, line)) {
+            const auto colon = line.find(" : ");
+            if (colon == std::string::npos || line.compare(0, colon, key) != 0 || colon != key.size()) continue;
+            std::istringstream vs(line.substr(colon + 3));
+            Tune u;
+            double m = 0.0;
+            if (vs >> u.x_rows >> u.y_tx >> u.la_tx >> u.tma >> u.nbuf >> u.pw >> m) c[key] = {u, m};
+        }
+        it = c.find(key);
+    }
+    if (it == c.end()) return false;
+    t = it->second.first;
+    ms = it->second.second;
+    return true;
+}
+
+static void tune_store(const std::string& key, const char* path, const Tune& t, double ms) {
+    tune_cache()[key] = {t, ms};
+    if (path && *path) {
+        std::ofstream out(path, std::ios::app);
+        out << key << " : " << t.x_rows << " " << t.y_tx << " " << t.la_tx << " " << t.tma << " " << t.nbuf << " "
+            << t.pw << " " << ms << "\n";
+    }
 }
 
 template <typename R>
@@ -927,6 +970,77 @@ class FieldT final : public Field {
         cudaEventDestroy(e1);
         graph_enabled_ = true;
         return ms;
+    }
+
+    double autotune(int nsteps, const char* cache_path, bool* from_cache) override {
+        if (nsteps < 1) throw std::invalid_argument("autotune needs nsteps >= 1");
+        const std::string key = tune_key();
+        Tune cached;
+        double cached_ms = 0.0;
+        if (tune_lookup(key, cache_path, cached, cached_ms)) {
+            tune_ = cached;
+            invalidate_graph();
+            if (from_cache) *from_cache = true;
+            return cached_ms;
+        }
+        // candidates: pencils per thread, ring depth, y / last-axis tile widths, rows per x block
+        std::vector<Tune> cands;
+        const int pws[2] = {sizeof(R) == 4 ? 2 : 1, 1};
+        for (int ip = 0; ip < (sizeof(R) == 4 ? 2 : 1); ++ip)
+            for (int nb : {0, 2, 4})
+                for (int ytx : {8, 16})
+                    for (int latx : {8, 16})
+                        for (int xr : {0, 4}) {
+                            Tune t;
+                            t.pw = pws[ip];
+                            t.nbuf = nb;
+                            t.y_tx = ytx;
+                            t.la_tx = latx;
+                            t.x_rows = xr;
+                            t.tma = 1;
+                            cands.push_back(t);
+                        }
+        // keep the state: tuning advances it
+        DevBuf save;
+        save.alloc(sizeof(C) * g_.S);
+        QX_CUDA(cudaMemcpyAsync(save.p, psi_.p, sizeof(C) * g_.S, cudaMemcpyDeviceToDevice, st_));
+        const Tune orig = tune_;
+        double best = 1e300;
+        Tune best_t = orig;
+        for (const Tune& t : cands) {
+            tune_ = t;
+            invalidate_graph();
+            try {
+                time_steps(1, 1);  // warm-up, capture
+                const double ms = time_steps(nsteps, 1) / nsteps;
+                if (ms < best) {
+                    best = ms;
+                    best_t = t;
+                }
+            } catch (const std::exception&) {
+                // a geometry this grid cannot launch (shared memory, tile width): skip it
+                cudaGetLastError();
+                QX_CUDA(cudaStreamSynchronize(st_));
+            }
+            QX_CUDA(cudaMemcpyAsync(psi_.p, save.p, sizeof(C) * g_.S, cudaMemcpyDeviceToDevice, st_));
+        }
+        QX_CUDA(cudaStreamSynchronize(st_));
+        if (best == 1e300) {
+            tune_ = orig;
+            invalidate_graph();
+            throw std::runtime_error("autotune: no candidate launch geometry ran");
+        }
+        tune_ = best_t;
+        invalidate_graph();
+        psi_changed();
+        tune_store(key, cache_path, best_t, best);
+        if (from_cache) *from_cache = false;
+        return best;
+    }
+
+    std::string tune_key() const {
+        return std::to_string(g_.dim) + " " + std::to_string(g_.N) + " " + (sizeof(R) == 4 ? "c64" : "c128") + " " +
+               std::to_string(g_.B);
     }
 
     // per-pass device time of the loop body, averaged over nsteps bodies

@@ -159,6 +159,12 @@ class Field {
 
     // ---- timing / device access ----
     virtual float time_steps(int nsteps, int use_graph) = 0;  // device ms of step(nsteps)
+    // Autotuner: time `nsteps` steps under each candidate launch geometry, keep
+    // the fastest (psi is restored afterwards).  Results are cached per (dim,
+    // N, precision, batch) in the process and, if `cache_path` is given, in
+    // that text file (read before tuning, appended after).  Returns the best
+    // ms per step; `from_cache` tells whether no timing was needed.
+    virtual double autotune(int nsteps, const char* cache_path, bool* from_cache) = 0;
     virtual void profile_step(int nsteps, std::vector<std::pair<std::string, double>>& per_kernel_ms) = 0;
     virtual void* psi_device() = 0;
     // psi was changed in place through psi_device(): drop derived state (V)
