@@ -404,6 +404,53 @@ def run_corrector(args, world, rank, local):
     corr.close()
 
 
+def run_report(args, world, rank, local):
+    """Error report of the fused FP32 form against the plain FP64 form (which
+    the GPU tests hold to <= 1e-12 of the CPU reference) for the 2D and 128^3
+    configurations: psi, potential, mass, energy and P(k) errors."""
+    if rank != 0:
+        return
+    import qaxions_b200 as qx
+    qx.set_device(local)
+    out = {}
+    for name, dim, N, ic, nsteps, every, nbins in (
+            ("2D 256^2, 8 Schive solitons, 500 steps, 64 linear P(k) bins every 50", 2, 256, qx.IC_SOLITONS, 500, 50, 64),
+            ("3D 128^3 GRF, 2000 steps, 64 linear P(k) bins every 200", 3, 128, qx.IC_GRF, 2000, 200, 64)):
+        dt = 0.2 / N**2
+        f = {}
+        for dtype in ("c128", "c64"):
+            g = qx.Field(dim, N, pref=1.0, dtype=dtype, k0="zero", dt=dt)
+            if ic == qx.IC_SOLITONS:
+                g.ic_config(ic, 1234, 8, 0.02, 0.05)
+            else:
+                g.ic_config(ic, 1234, 0, 0.01, 0.03)
+            f[dtype] = g
+        M0, E0, _, _ = f["c128"].mass_energy()
+        pk_err = 0.0
+        done = 0
+        while done < nsteps:
+            for g in f.values():
+                g.step(every)
+            done += every
+            _, pa, ca = f["c128"].spectrum(0, qx.SPEC_LINEAR, nbins)
+            _, pb, _ = f["c64"].spectrum(0, qx.SPEC_LINEAR, nbins)
+            sel = (ca > 0) & (pa > 1e-12 * pa.max())
+            pk_err = max(pk_err, float(np.max(np.abs(pb[sel] - pa[sel]) / pa[sel])))
+        a, b = f["c128"], f["c64"]
+        Ma, Ea, _, _ = a.mass_energy()
+        Mb, Eb, _, _ = b.mass_energy()
+        Va, Vb = a.V, b.V
+        out[name] = {
+            "relL2_psi": float(np.linalg.norm(b.psi - a.psi) / np.linalg.norm(a.psi)),
+            "relL2_V": float(np.linalg.norm((Vb - Vb.mean()) - (Va - Va.mean())) / np.linalg.norm(Va - Va.mean())),
+            "mass_drift_fp32": abs(Mb - M0) / M0, "mass_drift_fp64": abs(Ma - M0) / M0,
+            "energy_drift_fp32": abs(Eb - E0) / abs(E0), "energy_drift_fp64": abs(Ea - E0) / abs(E0),
+            "Pk_max_rel_err": pk_err}
+        for g in f.values():
+            g.close()
+    print(json.dumps({"metric": "FP32 (fused) vs FP64 (plain) error report", "configs": out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,13 +459,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--accuracy-steps", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="kdk512", choices=["kdk512", "ensemble", "corrector"],
+    ap.add_argument("--workload", default="kdk512", choices=["kdk512", "ensemble", "corrector", "report"],
                     help="kdk512: the 512^3 single-box step (default); ensemble: 16x64^3 + 16x96^3 + 16x128^3 "
                          "boxes; corrector: learned-corrector form at 256^3")
     ap.add_argument("--corr-pairs", type=int, default=8, help="training pairs per seed (corrector workload)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
+    if args.workload == "report" and args.impl == "ours":
+        run_report(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "corrector" and args.impl == "ours":
         run_corrector(args, world, rank, local)
         if world > 1:
