@@ -148,6 +148,8 @@ int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 int qx_copy_psi(qx_field_t *dst, qx_field_t *src);
 /* psi was written through qx_device_pointers: recompute V before it is used */
 int qx_psi_changed(qx_field_t *h);
+/* set the step counter and time (restoring a checkpoint) */
+int qx_set_clock(qx_field_t *h, int step, double time);
 /* psi *= factor (real) */
 int qx_scale_psi(qx_field_t *h, double factor);
 int qx_sync(qx_field_t *h);

@@ -78,6 +78,7 @@ _SIGS = {
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
     "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
+    "qx_set_clock": ([_vp, _i, _d], _i),
     "qx_ens_create": ([_i, _ip, _ip, _i, _d, _d, _i, _d, C.POINTER(_vp)], _i),
     "qx_ens_destroy": ([_vp], _i),
     "qx_ens_last_error": ([_vp], C.c_char_p),
@@ -146,6 +147,7 @@ class Field:
         _check(_lib.qx_create(dim, N, L, pref, rho_mean, QX_C128 if dtype == "c128" else QX_C64,
                               QX_K0_REFERENCE if k0 == "reference" else QX_K0_ZERO, dt, C.byref(self._h)))
         self.N_, self.dim_, self.L, self.dtype = N, dim, L, dtype
+        self._dt = dt
         self.shape = (N,) * dim
         self.hshape = (N,) * (dim - 1) + (N // 2 + 1,)
 
@@ -203,6 +205,10 @@ class Field:
 
     def set_dt(self, dt: float):
         self._c("qx_set_dt", dt)
+        self._dt = dt
+
+    def dt(self) -> float:
+        return self._dt
 
     # -- buffers --
     @property
@@ -358,6 +364,10 @@ class Field:
         persistent or the direct-load strided kernels (-1 keeps the current);
         pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
         self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
+
+    def set_clock(self, step: int, time: float):
+        """Set the step counter and time (restoring a checkpoint)."""
+        self._c("qx_set_clock", step, time)
 
     def autotune(self, nsteps: int = 3, cache: str | None = None):
         """Pick the fastest launch geometry for this grid (psi is left as it

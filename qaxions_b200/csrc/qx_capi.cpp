@@ -317,6 +317,13 @@ int qx_autotune(qx_field_t* h, int nsteps, const char* cache_path, double* best_
     });
 }
 
+int qx_set_clock(qx_field_t* h, int step, double time) {
+    return guarded(h, [&](qx::Field& f) {
+        need(step >= 0 && std::isfinite(time), "step must be >= 0 and time finite");
+        f.set_clock(step, time);
+    });
+}
+
 int qx_psi_changed(qx_field_t* h) {
     return guarded(h, [&](qx::Field& f) { f.psi_changed(); });
 }

@@ -190,6 +190,11 @@ class Field {
     double a() const { return a_; }
     double dt() const { return ds_; }
     void set_dt(double dt) { ds_ = dt; }
+    // restore the step counter and time of a checkpoint
+    void set_clock(int step, double time) {
+        curr_ = step;
+        s_ = time;
+    }
     Tune& tune() { return tune_; }
     // drop the captured loop-body graph (after launch geometry changes)
     virtual void invalidate_graph() = 0;
