@@ -148,6 +148,11 @@ int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 int qx_copy_psi(qx_field_t *dst, qx_field_t *src);
 /* psi was written through qx_device_pointers: recompute V before it is used */
 int qx_psi_changed(qx_field_t *h);
+/* cosmology: 0 STATIC (a = 1, the default); 1 MRE starting at a = ai:
+ * ds = dt / ai, norm 1 (Poisson prefactor a), rho_mean = 1.5 (2 pi)^2 1.27^2,
+ * and every step ds = 0.00025 / a, a *= 1 + 1.27^2 sqrt(1 + a) ds
+ * (src/field.cxx:70-90, 349-361).  MRE steps run without the loop-body graph. */
+int qx_set_cosmology(qx_field_t *h, int cosmo, double ai);
 /* set the step counter and time (restoring a checkpoint) */
 int qx_set_clock(qx_field_t *h, int step, double time);
 /* psi *= factor (real) */

@@ -49,6 +49,8 @@ def lib():
             "ref_vmax": ([vp], d),
             "ref_rhomax": ([vp], d),
             "ref_time": ([vp], d),
+            "ref_a": ([vp], d),
+            "ref_create_mre": ([i, i, d, d, d, i], vp),
             "ref_curr": ([vp], i),
             "ref_run": ([vp, i], None),
             "ref_loop_body": ([vp, i], None),
@@ -76,11 +78,15 @@ class RefField:
     norm is the reference's --norm: pref = 4 pi norm (src/field.cxx:78)."""
 
     def __init__(self, dim: int, N: int, L: float = 1.0, norm: float = 1.0, dt: float = 1e-4,
-                 nthr: int = 1):
+                 nthr: int = 1, mre_ai: float | None = None):
+        """mre_ai: build the MRE cosmology (src/field.cxx:82-88) starting at a = mre_ai."""
         self.dim, self.N = dim, N
         self.shape = (N,) * dim
         self.hshape = (N,) * (dim - 1) + (N // 2 + 1,)
-        self.h = lib().ref_create(dim, N, L, norm, dt, nthr)
+        if mre_ai is None:
+            self.h = lib().ref_create(dim, N, L, norm, dt, nthr)
+        else:
+            self.h = lib().ref_create_mre(dim, N, L, dt, mre_ai, nthr)
 
     def close(self):
         if self.h:

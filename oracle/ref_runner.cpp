@@ -55,6 +55,28 @@ void* ref_create(int dim, int N, double L, double norm, double dt, int nthr) {
     return h;
 }
 
+// MRE cosmology (src/field.cxx:82-88): a = ai, ds = dt / ai, norm 1,
+// rho_mean = 1.5 (2 pi)^2 1.27^2; updateTime advances a (src/field.cxx:349-361)
+void* ref_create_mre(int dim, int N, double L, double dt, double ai, int nthr) {
+    auto* h = new RefHandle();
+    defaults(h->pars);
+    h->pars.N = N;
+    h->pars.dim = dim;
+    h->pars.Lbox = L;
+    h->pars.norm = 1.0;
+    h->pars.dt = dt;
+    h->pars.ai = ai;
+    h->pars.nthr = nthr > 0 ? nthr : 1;
+    h->pars.verb = false;
+    h->pars.plan = FFTPlanType::ESTIMATE;
+    h->pars.cosmotype = CosmoType::MRE;
+    h->pars.measinfo = MeasureType::NONE;
+    omp_set_num_threads(h->pars.nthr);
+    initProfilers();
+    h->field = std::make_unique<Field>(h->pars);
+    return h;
+}
+
 void ref_destroy(void* p) { delete static_cast<RefHandle*>(p); }
 
 static Field& F(void* p) { return *static_cast<RefHandle*>(p)->field; }
@@ -98,6 +120,7 @@ void ref_propagate(void* p) { F(p).propagate(); }
 double ref_vmax(void* p) { return F(p).Vmax(); }
 double ref_rhomax(void* p) { return F(p).rhomax(); }
 double ref_time(void* p) { return F(p).time(); }
+double ref_a(void* p) { return F(p).a(); }
 int ref_curr(void* p) { return F(p).curr(); }
 
 // src/main.cxx:64-85 with measinfo = NONE: potential, half kick, then

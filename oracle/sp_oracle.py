@@ -126,6 +126,30 @@ def run(psi: np.ndarray, dt: float, nsteps: int, pref: float, rho_mean: float = 
     return psi, V
 
 
+MRE_RHO_MEAN = 1.5 * (2.0 * math.pi) ** 2 * 1.27 * 1.27
+
+
+def run_mre(psi: np.ndarray, dt: float, ai: float, nsteps: int, L: float = 1.0):
+    """Merged loop of src/main.cxx:64-85 in the MRE cosmology: a = ai,
+    ds = dt / ai, pref = norm a with norm 1, rho_mean = 1.5 (2 pi)^2 1.27^2
+    (src/field.cxx:82-88); updateTime after every drift sets ds = 0.00025 / a
+    and a *= 1 + 1.27^2 sqrt(1 + a) ds (src/field.cxx:349-361); the kick after
+    a drift uses the new ds.  Returns (psi, a, steps)."""
+    a = ai
+    ds = dt / ai
+    V, _ = update_potential(psi, a, MRE_RHO_MEAN, L, "reference")
+    psi = kick(psi, V, 0.5 * ds)
+    for i in range(nsteps):
+        psi = drift(psi, ds, L)
+        ds = 0.00025 / a
+        a = a * (1 + 1.27 * 1.27 * math.sqrt(1 + a) * ds)
+        V, _ = update_potential(psi, a, MRE_RHO_MEAN, L, "reference")
+        if i != nsteps - 1:
+            psi = kick(psi, V, ds)
+    psi = kick(psi, V, 0.5 * ds)
+    return psi, a, nsteps
+
+
 def kdk_step(psi: np.ndarray, dt: float, pref: float, rho_mean: float = 1.0, L: float = 1.0,
              k0: str = "reference"):
     """Unmerged step of src/examples/fieldtest.cxx:73-96 / Field::propagate

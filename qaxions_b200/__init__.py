@@ -79,6 +79,7 @@ _SIGS = {
     "qx_sync": ([_vp], _i),
     "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
     "qx_set_clock": ([_vp, _i, _d], _i),
+    "qx_set_cosmology": ([_vp, _i, _d], _i),
     "qx_ens_create": ([_i, _ip, _ip, _i, _d, _d, _i, _d, C.POINTER(_vp)], _i),
     "qx_ens_destroy": ([_vp], _i),
     "qx_ens_last_error": ([_vp], C.c_char_p),
@@ -364,6 +365,10 @@ class Field:
         persistent or the direct-load strided kernels (-1 keeps the current);
         pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
         self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
+
+    def set_cosmology(self, cosmo: int, ai: float = 1.0):
+        """0: STATIC; 1: MRE from a = ai (the reference's --cosmo mre)."""
+        self._c("qx_set_cosmology", cosmo, ai)
 
     def set_clock(self, step: int, time: float):
         """Set the step counter and time (restoring a checkpoint)."""

@@ -317,6 +317,10 @@ int qx_autotune(qx_field_t* h, int nsteps, const char* cache_path, double* best_
     });
 }
 
+int qx_set_cosmology(qx_field_t* h, int cosmo, double ai) {
+    return guarded(h, [&](qx::Field& f) { f.set_cosmology(cosmo, ai); });
+}
+
 int qx_set_clock(qx_field_t* h, int step, double time) {
     return guarded(h, [&](qx::Field& f) {
         need(step >= 0 && std::isfinite(time), "step must be >= 0 and time finite");

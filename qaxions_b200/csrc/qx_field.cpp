@@ -287,9 +287,31 @@ template class B200FFTBackend<double>;
 // Field
 // ---------------------------------------------------------------------------
 
-void Field::updateTime() {  // src/field.cxx:349-361 (STATIC cosmology: a = 1)
+void Field::updateTime() {  // src/field.cxx:349-361
     curr_ += 1;
+    if (cosmo_ == 1) {  // MRE: the step follows a, then a advances
+        ds_ = 0.00025 / a_;
+        a_ = a_ * (1 + 1.27 * 1.27 * std::sqrt(1 + a_) * ds_);
+    }
     s_ += ds_;
+}
+
+void Field::set_cosmology(int cosmo, double ai) {  // src/field.cxx:70-90
+    if (cosmo == 0) {
+        cosmo_ = 0;
+        a_ = 1.0;
+        ds_ = cfg_.dt;
+    } else if (cosmo == 1) {
+        if (!(ai > 0)) throw std::invalid_argument("MRE needs ai > 0");
+        cosmo_ = 1;
+        a_ = ai;
+        ds_ = cfg_.dt / ai;
+        s_ = 0.0;  // the reference leaves s unset here
+        cfg_.rho_mean = 1.5 * kTwoPi * kTwoPi * 1.27 * 1.27;
+    } else {
+        throw std::invalid_argument("cosmology must be 0 (STATIC) or 1 (MRE)");
+    }
+    invalidate_graph();
 }
 
 void Field::drift_update() {  // src/field.cxx:378-386
@@ -447,7 +469,7 @@ class FieldT final : public Field {
         auto a = xp();
         a.in = psi();
         a.vh = vh();
-        a.pref = cfg_.pref;
+        a.pref = pref_eff();
         a.rho_mean = cfg_.rho_mean;
         Ops<R>::x_r2c(g_.N, a, false, tune_, st_);
         y_fwd(vh(), g_.N / 2);
@@ -508,24 +530,38 @@ class FieldT final : public Field {
             a.dt = 0.5 * ds_;
             Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_);
         }
-        // body: psi^_x -> drift -> psi, rho^ -> Poisson -> kick -> psi^_x
-        for (int i = 0; i < nsteps - 1; ++i) {
-            if (graph_enabled_) {
-                if (!graph_exec_ || graph_dt_ != ds_) capture_body();
-                QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
-            } else {
-                body(ds_, false);
+        if (cosmo_ == 1) {
+            // MRE: every step has its own drift step, prefactor (norm a) and
+            // kick step (after updateTime), so the body runs without the graph
+            for (int i = 0; i < nsteps; ++i) {
+                const double dt_drift = ds_;
+                updateTime();
+                body(dt_drift, ds_, pref_eff(), i == nsteps - 1);
             }
+        } else {
+            // body: psi^_x -> drift -> psi, rho^ -> Poisson -> kick -> psi^_x
+            for (int i = 0; i < nsteps - 1; ++i) {
+                if (graph_enabled_) {
+                    if (!graph_exec_ || graph_dt_ != ds_) capture_body();
+                    QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
+                } else {
+                    body(ds_, ds_, pref_eff(), false);
+                }
+            }
+            body(ds_, ds_, pref_eff(), true);
+            curr_ += nsteps;
+            s_ += nsteps * ds_;
         }
-        body(ds_, true);
-        curr_ += nsteps;
-        s_ += nsteps * ds_;
         v_current_ = true;
         vmax_stale_ = true;
     }
 
+    // Poisson source prefactor: pref (STATIC) or norm a with norm = 1 (MRE,
+    // src/field.cxx:84-86,298)
+    double pref_eff() const { return cosmo_ == 1 ? a_ : cfg_.pref; }
+
     // one loop iteration; last = final half kick, psi in real space, V written
-    void body(double dt, bool last) {
+    void body(double dt, double dt_kick, double pref, bool last) {
         y_fwd(psi(), g_.N);
         la_drift(dt);
         y_inv(psi(), g_.N);
@@ -534,17 +570,17 @@ class FieldT final : public Field {
         a.out = psi();
         a.vh = vh();
         a.Vout = V();
-        a.pref = cfg_.pref;
+        a.pref = pref;
         a.rho_mean = cfg_.rho_mean;
         Ops<R>::x_inv(g_.N, a, true, tune_, st_);
         y_fwd(vh(), g_.N / 2);
         la_poisson();
         y_inv(vh(), g_.N / 2);
         if (last) {
-            a.dt = 0.5 * dt;
+            a.dt = 0.5 * dt_kick;
             Ops<R>::x_c2r(g_.N, a, C2R_WRITE_V | C2R_KICK | C2R_WRITE_PSI, tune_, st_);
         } else {
-            a.dt = dt;
+            a.dt = dt_kick;
             Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_);
         }
     }
@@ -556,7 +592,7 @@ class FieldT final : public Field {
         cudaGraph_t g;
         QX_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
         try {
-            body(ds_, false);
+            body(ds_, ds_, pref_eff(), false);
         } catch (...) {
             cudaStreamEndCapture(st_, &g);
             if (g) cudaGraphDestroy(g);
@@ -1074,7 +1110,7 @@ class FieldT final : public Field {
             if (d3) { y_inv(psi(), g_.N); mark(); }
             auto a = xp();
             a.in = psi(); a.out = psi(); a.vh = vh(); a.Vout = V();
-            a.pref = cfg_.pref; a.rho_mean = cfg_.rho_mean; a.dt = ds_;
+            a.pref = pref_eff(); a.rho_mean = cfg_.rho_mean; a.dt = ds_;
             Ops<R>::x_inv(g_.N, a, true, tune_, st_); mark();
             if (d3) { y_fwd(vh(), g_.N / 2); mark(); }
             la_poisson(); mark();

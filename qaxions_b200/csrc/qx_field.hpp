@@ -116,6 +116,9 @@ class Field {
     virtual void updatePotential() = 0;
     virtual void computeEnergy() = 0;     // reference semantics: V <- |psi|^2, rhomax
     void updateTime();
+    // 0: STATIC (a = 1); 1: MRE from a = ai (src/field.cxx:70-90, 349-361)
+    void set_cosmology(int cosmo, double ai);
+    int cosmology() const { return cosmo_; }
     void half_kick() { kick(0.5 * ds_); }
     void full_kick() { kick(ds_); }
     void drift_update();
@@ -207,6 +210,7 @@ class Field {
     int curr_ = 0;
     double s_ = 0.0, a_ = 1.0, ds_ = 0.0;
     double vmax_ = 0.0, rhomax_ = 0.0;
+    int cosmo_ = 0;
 };
 
 std::unique_ptr<Field> make_field(const FieldConfig& cfg);

@@ -17,6 +17,7 @@ project FFTW shim -- from a directory holding the reference's solitons.txt
                      module returns
   golden_ic.npz      the synthetic benchmark ICs from the NumPy oracle
                      (no reference counterpart), small sizes
+  golden_mre.npz     the merged loop in the MRE cosmology (make_mre)
 
 Nothing at test time reads the reference tree.
 """
@@ -38,6 +39,35 @@ from oracle import ref_lib as R  # noqa: E402
 from oracle import sp_oracle as O  # noqa: E402
 
 REF_SOLITONS = "/root/reference/solitons.txt"
+
+
+def make_mre():
+    """golden_mre.npz: the merged loop in the reference's MRE cosmology
+    (src/field.cxx:82-88, 349-361), a_i = 0.1, 10 steps from the soliton IC."""
+    work = tempfile.mkdtemp()
+    shutil.copy(REF_SOLITONS, os.path.join(work, "solitons.txt"))
+    cwd = os.getcwd()
+    os.chdir(work)
+    try:
+        out = {}
+        for dim, N in [(2, 32), (3, 16)]:
+            tag = f"d{dim}_n{N}"
+            f = R.RefField(dim, N, 1.0, 1.0, 0.05)
+            f.ic_solitons(1.0)
+            psi0 = f.psi()
+            dt = 1e-3
+            g = R.RefField(dim, N, 1.0, 1.0, dt, mre_ai=0.1)
+            g.set_psi(psi0)
+            g.run(10)
+            out[f"{tag}_psi0"] = psi0
+            out[f"{tag}_dt"] = np.float64(dt)
+            out[f"{tag}_ai"] = np.float64(0.1)
+            out[f"{tag}_psi_run"] = g.psi()
+            out[f"{tag}_a_run"] = np.float64(R.lib().ref_a(g.h))
+            out[f"{tag}_curr_run"] = np.int64(R.lib().ref_curr(g.h))
+        np.savez_compressed(os.path.join(HERE, "golden_mre.npz"), **out)
+    finally:
+        os.chdir(cwd)
 
 
 def main():
@@ -142,4 +172,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["mre"]:
+        make_mre()
+    else:
+        main()
+        make_mre()

@@ -328,3 +328,21 @@ def test_fp32_kick_accuracy():
         err = np.abs(got - ref) / np.abs(psi)
         assert err.max() < 4e-7, (dt, vmax, err.max())
     f.close()
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_mre_cosmology_matches_reference(dtype):
+    """The merged loop in the MRE cosmology against the reference's own run
+    (tests/golden/golden_mre.npz): psi, the scale factor and the step count."""
+    d = np.load(os.path.join(GOLDEN, "golden_mre.npz"))
+    for dim, N in ((2, 32), (3, 16)):
+        tag = f"d{dim}_n{N}"
+        f = qx.Field(dim, N, pref=1.0, dtype=dtype, k0="reference", dt=float(d[f"{tag}_dt"]))
+        f.set_cosmology(1, float(d[f"{tag}_ai"]))
+        f.psi = d[f"{tag}_psi0"]
+        f.step(10)
+        assert f.curr() == int(d[f"{tag}_curr_run"])
+        assert abs(f.a() - float(d[f"{tag}_a_run"])) <= 1e-15
+        err = O.rel_l2(f.psi, d[f"{tag}_psi_run"])
+        assert err <= (1e-12 if dtype == "c128" else 1e-5), (tag, err)
+        f.close()

@@ -127,3 +127,13 @@ def test_live_reference_matches_oracle(soliton_dir):
         psi, V = O.run(psi0, 0.01, 5, PREF)
         assert O.rel_l2(psi, f.psi()) < 1e-13
         f.close()
+
+
+def test_mre_restatement_matches_reference_golden():
+    """The MRE merged loop of the restatement against the reference's own run."""
+    d = np.load(os.path.join(GOLDEN, "golden_mre.npz"))
+    for tag in ("d2_n32", "d3_n16"):
+        psi, a, n = O.run_mre(d[f"{tag}_psi0"], float(d[f"{tag}_dt"]), float(d[f"{tag}_ai"]), 10)
+        assert abs(a - float(d[f"{tag}_a_run"])) <= 1e-15
+        assert n == int(d[f"{tag}_curr_run"])
+        assert O.rel_l2(psi, d[f"{tag}_psi_run"]) <= 1e-12
