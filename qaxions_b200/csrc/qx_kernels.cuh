@@ -116,9 +116,17 @@ template <typename C> __device__ __forceinline__ C cmul_d(C v, double2 w) {
     return mk<C>((decltype(C::x))fma(vx, w.x, -vy * w.y), (decltype(C::x))fma(vx, w.y, vy * w.x));
 }
 
-// psi * exp(-i dt V)   (src/field.cxx:100-112)
-template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, double dt) {
-    return cmul(p, cis<R>(-dt * (double)v));
+// psi * exp(-i dt V)   (src/field.cxx:100-112).  FP64: phase reduced mod 2 pi
+// in FP64.  FP32: the phase -dt V is formed in FP32 (one rounding, the size of
+// V's own FP32 representation error) and reduced by sincosf itself.
+template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, double dt);
+template <> __device__ __forceinline__ double2 kick1<double>(double2 p, double v, double dt) {
+    return cmul(p, cis<double>(-dt * v));
+}
+template <> __device__ __forceinline__ float2 kick1<float>(float2 p, float v, double dt) {
+    float s, c;
+    sincosf((float)(-dt) * v, &s, &c);
+    return cmul(p, make_float2(c, s));
 }
 
 __device__ __forceinline__ int signed_mode(int i, int N) { return i <= (N >> 1) ? i : i - N; }
@@ -404,8 +412,25 @@ enum XC2RFlags {
     XC_FWD = 8,        // forward x FFT of the kicked psi -> out
 };
 
+// cp.async 16-byte copy global -> shared (no register round trip) and its groups
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// staging buffer of a kicking c2r row pass (FP32): next row's vh (N/2) and psi (N)
+template <int N, typename R, int FLAGS> __host__ __device__ constexpr int x_c2r_stage_elems() {
+    return (sizeof(R) == 4 && (FLAGS & 2)) ? N / 2 + N : 0;
+}
+
 // c2r along x of the packed vh rows -> V (unnormalised, FFTW convention);
 // then optionally kick psi by V (dt), store psi, or forward-transform it.
+// FP32 kicking passes are software-pipelined: after its kick, a warp copies
+// its next row's vh and psi into a per-warp staging buffer with cp.async, so
+// they arrive while the forward transform and stores of the current row run.
 template <int N, typename R, int FLAGS>
 __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     using C = cx_t<R>;
@@ -413,27 +438,53 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
     constexpr int T = qx_row_threads(N);
+    constexpr int SE = x_c2r_stage_elems<N, R, FLAGS>();
+    constexpr bool STAGE = SE > 0;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     XTabs<C> tb;
     C* sm = x_setup<N, R>(a, smem_raw, tb);
     const int t = threadIdx.x;
     RowAcc<C> acc{sm, warp_lanes_mask()};
+    // staging after all P row buffers (16-byte aligned for cp.async)
+    C* stg = reinterpret_cast<C*>(
+                 (reinterpret_cast<uintptr_t>(sm - threadIdx.y * row_smem_elems(N) + blockDim.y * row_smem_elems(N)) +
+                  15) & ~(uintptr_t)15) +
+             threadIdx.y * SE;
+    auto prefetch = [&](long r) {
+        if constexpr (STAGE) {
+            const char* gv = reinterpret_cast<const char*>(a.vh + r * M);
+            const char* gp = reinterpret_cast<const char*>(a.in + r * N);
+            char* sv = reinterpret_cast<char*>(stg);
+            char* sp = reinterpret_cast<char*>(stg + M);
+            for (int i = t; i < (int)(M * sizeof(C) / 16); i += T) cp_async16(sv + 16 * i, gv + 16 * i);
+            for (int i = t; i < (int)(N * sizeof(C) / 16); i += T) cp_async16(sp + 16 * i, gp + 16 * i);
+            cp_async_commit();
+        }
+    };
+    if (x_row0() < a.rows) prefetch(x_row0());
     for (long row = x_row0(); row < a.rows; row += x_row_step()) {
         acc.sync();
-        const C* hrow = a.vh + row * M;
+        if constexpr (STAGE) {
+            cp_async_wait_all();
+            acc.sync();
+        } else {
+            const C* hrow = a.vh + row * M;
 #pragma unroll
-        for (int i = 0; i < M / T; ++i) acc(t + i * T) = hrow[t + i * T];
-        acc.sync();
+            for (int i = 0; i < M / T; ++i) acc(t + i * T) = hrow[t + i * T];
+            acc.sync();
+        }
+        // the vh row: staged copy (FP32 kicking passes) or the row buffer
+        auto hv = [&](int k) -> C { return STAGE ? stg[k] : acc(k); };
         C z[EH];
 #pragma unroll
         for (int e = 0; e < EH; ++e) {
             const int k = out_pos<M, EH>(e, t);
-            const C X = acc(k);
+            const C X = hv(k);
             if (k == 0) {
                 // X[0] = Re col0, X[N/2] = Im col0
                 z[e] = mk<C>(X.x + X.y, X.x - X.y);
             } else {
-                const C B = cconj(acc(M - k));
+                const C B = cconj(hv(M - k));
                 const C s = cadd(X, B), d = csub(X, B);
                 const C w = cconj(tb.Nn[k]);  // W_N^{-k}
                 const C wd = cmul(w, d);
@@ -453,9 +504,15 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
 #pragma unroll
             for (int e = 0; e < EH; ++e) {
                 C p0, p1;
-                load_pair(a.in + row * N, in_pos<M, EH, 0>(e, t), p0, p1);
+                load_pair(STAGE ? stg + M : a.in + row * N, in_pos<M, EH, 0>(e, t), p0, p1);
                 ps[row_pair_idx<N>(e, 0)] = kick1<R>(p0, z[e].x, a.dt);
                 ps[row_pair_idx<N>(e, 1)] = kick1<R>(p1, z[e].y, a.dt);
+            }
+            if constexpr (STAGE) {
+                // every lane is done with the staged row: fetch the next one
+                acc.sync();
+                const long nrow = row + x_row_step();
+                if (nrow < a.rows) prefetch(nrow);
             }
             if constexpr (FLAGS & XC_WRITE_PSI) {
 #pragma unroll

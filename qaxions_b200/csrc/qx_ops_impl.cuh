@@ -93,10 +93,12 @@ static int sm_count() {
 }
 
 template <typename R, int NN, typename K>
-static void launch_x(K kernel, const XArgs<R>& x, int P, cudaStream_t st) {
+static void launch_x(K kernel, const XArgs<R>& x, int P, cudaStream_t st, int stage_elems = 0) {
     using C = cx_t<R>;
     const int T = qx_row_threads(NN);
-    const size_t smem = ((size_t)x_table_elems<NN, R>() + (size_t)P * row_smem_elems(NN)) * sizeof(C);
+    // tables + P row buffers (+ P staging buffers and alignment slack)
+    const size_t smem = ((size_t)x_table_elems<NN, R>() + (size_t)P * row_smem_elems(NN) +
+                         (stage_elems ? (size_t)P * stage_elems + 2 : 0)) * sizeof(C);
     set_smem(kernel, smem);
     // persistent grid: as many blocks as fit on the device at once (the
     // twiddle tables are staged once per block), at most one per P rows
@@ -159,11 +161,18 @@ void Ops<R>::x_c2r(int N, const XP& a, int flags, const Tune& tu, cudaStream_t s
     QX_FOR_N(N, {
         switch (flags) {
             case C2R_WRITE_V: launch_x<R, NN>(k_x_c2r<NN, R, XC_WRITE_V>, x, P, st); break;
-            case C2R_KICK | C2R_FWD: launch_x<R, NN>(k_x_c2r<NN, R, XC_KICK | XC_FWD>, x, P, st); break;
+            case C2R_KICK | C2R_FWD:
+                launch_x<R, NN>(k_x_c2r<NN, R, XC_KICK | XC_FWD>, x, P, st,
+                                x_c2r_stage_elems<NN, R, XC_KICK | XC_FWD>());
+                break;
             case C2R_WRITE_V | C2R_KICK | C2R_FWD:
-                launch_x<R, NN>(k_x_c2r<NN, R, XC_WRITE_V | XC_KICK | XC_FWD>, x, P, st); break;
+                launch_x<R, NN>(k_x_c2r<NN, R, XC_WRITE_V | XC_KICK | XC_FWD>, x, P, st,
+                                x_c2r_stage_elems<NN, R, XC_WRITE_V | XC_KICK | XC_FWD>());
+                break;
             case C2R_WRITE_V | C2R_KICK | C2R_WRITE_PSI:
-                launch_x<R, NN>(k_x_c2r<NN, R, XC_WRITE_V | XC_KICK | XC_WRITE_PSI>, x, P, st); break;
+                launch_x<R, NN>(k_x_c2r<NN, R, XC_WRITE_V | XC_KICK | XC_WRITE_PSI>, x, P, st,
+                                x_c2r_stage_elems<NN, R, XC_WRITE_V | XC_KICK | XC_WRITE_PSI>());
+                break;
             default: throw std::invalid_argument("x_c2r: unsupported flag combination");
         }
     });
