@@ -247,6 +247,22 @@ __device__ __forceinline__ cx_t<R>* x_setup(const XArgs<R>& a, unsigned char* sm
 __device__ __forceinline__ long x_row0() { return (long)blockIdx.x * blockDim.y + threadIdx.y; }
 __device__ __forceinline__ long x_row_step() { return (long)gridDim.x * blockDim.y; }
 
+// cp.async 16-byte copy global -> shared (no register round trip) and its groups
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+
+// per-warp staging buffer after the P row buffers (16-byte aligned for cp.async)
+template <int N, typename C> __device__ __forceinline__ C* x_stage_ptr(C* row_buf, int stage_elems) {
+    C* end = row_buf - threadIdx.y * row_smem_elems(N) + blockDim.y * row_smem_elems(N);
+    return reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(end) + 15) & ~(uintptr_t)15) + threadIdx.y * stage_elems;
+}
+
 enum XFwdMode { XF_PLAIN = 0, XF_KICK = 1 };
 
 // forward c2c along x; optional kick by V first.  (Field::kick + first FFT pass)
@@ -412,15 +428,6 @@ enum XC2RFlags {
     XC_FWD = 8,        // forward x FFT of the kicked psi -> out
 };
 
-// cp.async 16-byte copy global -> shared (no register round trip) and its groups
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
-                 "l"(gmem_src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 // staging buffer of a kicking c2r row pass (FP32): next row's vh (N/2) and psi (N)
 template <int N, typename R, int FLAGS> __host__ __device__ constexpr int x_c2r_stage_elems() {
     return (sizeof(R) == 4 && (FLAGS & 2)) ? N / 2 + N : 0;
@@ -445,11 +452,7 @@ __global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
     C* sm = x_setup<N, R>(a, smem_raw, tb);
     const int t = threadIdx.x;
     RowAcc<C> acc{sm, warp_lanes_mask()};
-    // staging after all P row buffers (16-byte aligned for cp.async)
-    C* stg = reinterpret_cast<C*>(
-                 (reinterpret_cast<uintptr_t>(sm - threadIdx.y * row_smem_elems(N) + blockDim.y * row_smem_elems(N)) +
-                  15) & ~(uintptr_t)15) +
-             threadIdx.y * SE;
+    C* stg = x_stage_ptr<N>(sm, SE);
     auto prefetch = [&](long r) {
         if constexpr (STAGE) {
             const char* gv = reinterpret_cast<const char*>(a.vh + r * M);
