@@ -214,7 +214,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
 // Tensor map over a complex [NZ][N][X] array viewed as reals [NZ][N][2X];
 // box = 2TX reals x `box` positions along dim 1 (pencil_dim 1) or dim 2.
 template <typename R>
-static CUtensorMap make_tmap(const void* base, int X, int N, int NZ, int TX, int box, int pencil_dim) {
+static CUtensorMap make_tmap(const void* base, int X, int N, int NZ, int TX, int box, int pencil_dim, bool swz = false) {
     CUtensorMap tm;
     cuuint64_t dims[3] = {(cuuint64_t)2 * X, (cuuint64_t)N, (cuuint64_t)NZ};
     cuuint64_t strides[2] = {(cuuint64_t)2 * X * sizeof(R), (cuuint64_t)2 * X * (cuuint64_t)N * sizeof(R)};
@@ -223,7 +223,8 @@ static CUtensorMap make_tmap(const void* base, int X, int N, int NZ, int TX, int
     cuuint32_t es[3] = {1, 1, 1};
     const CUresult r = tmap_encoder()(&tm, sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                                       3, const_cast<void*>(base), dims, strides, boxd, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                      swz ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return tm;
@@ -304,9 +305,10 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.col0_external = col0_ext;
     s.partial = a.partial;
     s.err = a.err;
-    const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim);
+    constexpr bool SWZ = tma_swizzled<NN, R, PW, TXF>();
+    const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim, SWZ);
     auto kern = k_pencil_tma<NN, R, OP, PW, DF, TXF>;
-    const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP);
+    const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP, SWZ);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
     const int key = g.nbuf * 8 + (g.TX == 16 ? 4 : g.TX == 8 ? 3 : g.TX == 4 ? 2 : g.TX == 2 ? 1 : 0);
@@ -317,7 +319,7 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     }
     long grid = (long)sm_count() * bps;
     if (grid > s.n_tiles) grid = s.n_tiles;
-    dim3 blk(g.TX / PW, g.T, 1);
+    dim3 blk(SWZ ? g.TX / PW / 2 : g.TX / PW, g.T, SWZ ? 2 : 1);
     kern<<<(unsigned)grid, blk, smem, st>>>(tm, s);
     QX_LAUNCH_CHECK();
     return grid;

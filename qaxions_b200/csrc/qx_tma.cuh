@@ -129,9 +129,11 @@ __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(s
 // dynamic shared memory of a pass: NBUF tiles + twiddles + drift factors
 // (drift only) + column-0 stash (Poisson only) + 128-byte base-alignment slack (the
 // tensor-copy alignment of unswizzled tiles; tiles are 1 KB multiples)
-template <typename R> __host__ __device__ constexpr size_t tma_smem_bytes(int N, int TX, int nbuf, int op) {
+template <typename R> __host__ __device__ constexpr size_t tma_smem_bytes(int N, int TX, int nbuf, int op,
+                                                                          bool swz = false) {
     return (size_t)nbuf * align1k((size_t)N * TX * 2 * sizeof(R)) + (size_t)N * 4 * sizeof(R) +
-           (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) + 128;
+           (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) +
+           (swz ? 1024 : 128);
 }
 
 template <typename R> struct TArgs {
@@ -151,7 +153,36 @@ template <typename R> struct TArgs {
     int* err;            // set to 1 when a wait timed out
 };
 
-// blockDim = (TX / PW, N / E): thread (c, t) owns columns x0 + PW c + h (h < PW);
+// 128-byte-row tiles of paired pencils (FP32, TX = 16, PW = 2): the tile is
+// stored with TMA's 128-byte swizzle (16-byte chunk index XOR row mod 8), so
+// the 16-byte pencil-pair accesses of a warp stay bank-conflict free, and the
+// block runs as two groups of 8 warps that synchronise their FFT exchanges
+// with named barriers (a group owns 4 of the 8 pencil pairs of every row).
+template <int N, typename R, int PW, int TXF> __host__ __device__ constexpr bool tma_swizzled() {
+    return sizeof(R) == 4 && PW == 2 && TXF == 16;
+}
+
+__device__ __forceinline__ void named_barrier(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// pencil group c of a tile: element p at base[p * pitch + c] (plain) or at
+// base[p * 8 + (c ^ (p & 7))] (swizzled 128-byte rows of 8 pairs)
+template <typename P, bool SWZ> struct TileAcc {
+    P* base;
+    int c, pitch;
+    __device__ __forceinline__ P& operator()(int p) const {
+        if constexpr (SWZ) return base[p * 8 + (c ^ (p & 7))];
+        else return base[p * pitch + c];
+    }
+    __device__ __forceinline__ void sync() const {
+        if constexpr (SWZ) named_barrier(1 + (int)threadIdx.z, (int)(blockDim.x * blockDim.y));
+        else __syncthreads();
+    }
+};
+
+// blockDim = (TX / PW, N / E, 1), or (TX / PW / 2, N / E, 2) when swizzled:
+// thread (c, t) owns columns x0 + PW c + h (h < PW), c = x + blockDim.x z;
 // TX = TXF when TXF > 0
 template <int N, typename R, int OP, int PW, bool DF, int TXF>
 __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_block_min<N, R, PW, TXF>()))
@@ -165,13 +196,16 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
     __shared__ int s_abort;
     __shared__ double red[32];
     const int TX = TXF > 0 ? TXF : s.TX;
+    constexpr bool SWZ = tma_swizzled<N, R, PW, TXF>();
     const int TG = TX / PW;  // pencil groups per tile row
-    const int c = threadIdx.x, t = threadIdx.y;
-    const int tid = c + TG * t;
-    const int nthr = TG * blockDim.y;
+    const int c = threadIdx.x + blockDim.x * threadIdx.z, t = threadIdx.y;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
     const uint32_t tile_bytes = (uint32_t)((size_t)N * TX * sizeof(C));
     const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
-    C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+    // tiles on 128-byte boundaries, 1024 for the 128-byte swizzle
+    constexpr uintptr_t BA = SWZ ? 1023 : 127;
+    C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + BA) & ~BA);
     C* tws = bufs + s.nbuf * tile_elems;
     C* tws_lo = tws + N;
     double2* bz = reinterpret_cast<double2*>(tws_lo + N);
@@ -232,7 +266,7 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         const int x0 = (int)(id % s.tiles_x) * TX;
         const int o = (int)(id / s.tiles_x);
         const int xb = x0 + PW * c;  // column of pencil 0 of this thread
-        ColAcc<P> acc{reinterpret_cast<P*>(tile) + c, TG};
+        TileAcc<P, SWZ> acc{reinterpret_cast<P*>(tile), c, TG};
         P v[E];
         if constexpr (OP == OP_INV) {
 #pragma unroll
