@@ -137,6 +137,15 @@ int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, dou
  * 0 = direct loads; -1 = keep), TMA ring depth, pencils per thread of the TMA
  * passes (1 or 2; 0 = default: 2 in the FP32 form, FP64 always 1) */
 int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw);
+/* Drift chain (no counterpart in the reference: the reference's drift,
+ * src/field.cxx:119-198, is three library FFT calls around a multiply).  on = 0
+ * (default): the y forward, z drift and y inverse passes of a 3D complex64
+ * field run as three persistent passes; on = 2 / 1: as one cooperative kernel
+ * that walks the array in x-slabs of 16 / 8 columns, so the later phases of a
+ * slab can read the earlier ones' output from L2.  Results are bit-identical
+ * in all three modes; on B200 the three passes are faster at every size
+ * measured (64^3 .. 512^3). */
+int qx_set_chain(qx_field_t *h, int on);
 /* Autotuner: time nsteps steps under each candidate launch geometry (pencils
  * per thread, TMA ring depth, tile widths, rows per x block), keep the fastest;
  * psi is restored afterwards.  Cached per (dim, N, dtype, batch) in the process

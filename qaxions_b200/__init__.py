@@ -75,6 +75,7 @@ _SIGS = {
     "qx_time_steps": ([_vp, _i, _i, _fp], _i),
     "qx_profile_step": ([_vp, _i, _i, C.c_char_p, _dp, _ip], _i),
     "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
+    "qx_set_chain": ([_vp, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
     "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
@@ -365,6 +366,13 @@ class Field:
         persistent or the direct-load strided kernels (-1 keeps the current);
         pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
         self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
+
+    def set_chain(self, on):
+        """Drift chain: the y, z-drift, y passes of a 3D complex64 field as
+        three passes (False / 0, the default, fastest) or as one slab-ordered
+        kernel over 16-column (True / 2) or 8-column (1) slabs; the results
+        are bit-identical."""
+        self._c("qx_set_chain", 2 if on is True else int(on))
 
     def set_cosmology(self, cosmo: int, ai: float = 1.0):
         """0: STATIC; 1: MRE from a = ai (the reference's --cosmo mre)."""

@@ -279,6 +279,14 @@ int qx_set_tune(qx_field_t* h, int x_rows, int y_tx, int la_tx, int tma, int nbu
     });
 }
 
+int qx_set_chain(qx_field_t* h, int on) {
+    return guarded(h, [&](qx::Field& f) {
+        need(on >= 0 && on <= 2, "chain must be 0, 1 or 2");
+        f.tune().chain = on;
+        f.invalidate_graph();
+    });
+}
+
 int qx_device_pointers(qx_field_t* h, void** psi, void** V) {
     return guarded(h, [&](qx::Field& f) {
         if (psi) *psi = f.psi_device();

@@ -421,6 +421,9 @@ class FieldT final : public Field {
         QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
         fft_ = std::make_unique<B200FFTBackend<R>>(g_, tw_, &tune_, st_, err_);
+        // drift chain: phase counters (as many as 8-column slabs need)
+        chain_n_ = Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, 1);
+        if (chain_n_) chain_.alloc(sizeof(unsigned) * 3 * (size_t)chain_n_);
         QX_CUDA(cudaStreamSynchronize(st_));
     }
 
@@ -457,6 +460,21 @@ class FieldT final : public Field {
         s.scale = 1.0 / (double)g_.S1;
         Ops<R>::la_pass(g_.N, s, OP_DRIFT, tune_, st_);
     }
+    // psi^_x -> y forward, z drift, y inverse: one slab-ordered kernel (FP32
+    // 3D, tune_.chain) or three passes
+    bool chain_on() const { return chain_n_ && tune_.tma && Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, tune_.chain); }
+    void yz_drift(double dt) {
+        if (chain_on()) {
+            auto s = sp(psi(), g_.N);
+            s.phase_fac = -0.5 * dt * dk() * dk();
+            s.scale = 1.0 / (double)g_.S1;
+            Ops<R>::drift_chain(g_.N, s, tune_.chain, chain_.as<unsigned>(), tune_, st_);
+            return;
+        }
+        y_fwd(psi(), g_.N);
+        la_drift(dt);
+        y_inv(psi(), g_.N);
+    }
     void la_poisson() {
         auto s = sp(vh(), g_.N / 2);
         s.pois_c = pois_c();
@@ -483,9 +501,7 @@ class FieldT final : public Field {
         a.in = psi();
         a.out = psi();
         Ops<R>::x_fwd(g_.N, a, false, tune_, st_);
-        y_fwd(psi(), g_.N);
-        la_drift(dt);
-        y_inv(psi(), g_.N);
+        yz_drift(dt);
         Ops<R>::x_inv(g_.N, a, false, tune_, st_);
         v_current_ = false;
     }
@@ -562,9 +578,7 @@ class FieldT final : public Field {
 
     // one loop iteration; last = final half kick, psi in real space, V written
     void body(double dt, double dt_kick, double pref, bool last) {
-        y_fwd(psi(), g_.N);
-        la_drift(dt);
-        y_inv(psi(), g_.N);
+        yz_drift(dt);
         auto a = xp();
         a.in = psi();
         a.out = psi();
@@ -1082,10 +1096,15 @@ class FieldT final : public Field {
     // per-pass device time of the loop body, averaged over nsteps bodies
     void profile_step(int nsteps, std::vector<std::pair<std::string, double>>& out) override {
         const bool d3 = g_.dim == 3;
+        const bool chain = chain_on();
         std::vector<std::string> names;
-        if (d3) names.push_back("y_fwd(psi)");
-        names.push_back(d3 ? "z_drift(psi)" : "y_drift(psi)");
-        if (d3) names.push_back("y_inv(psi)");
+        if (chain) {
+            names.push_back("yzy_drift_chain(psi)");
+        } else {
+            if (d3) names.push_back("y_fwd(psi)");
+            names.push_back(d3 ? "z_drift(psi)" : "y_drift(psi)");
+            if (d3) names.push_back("y_inv(psi)");
+        }
         names.push_back("x_inv_r2c(psi->rho^)");
         if (d3) names.push_back("y_fwd(rho^)");
         names.push_back(d3 ? "z_poisson(rho^)" : "y_poisson(rho^)");
@@ -1105,9 +1124,13 @@ class FieldT final : public Field {
             size_t k = 0;
             QX_CUDA(cudaEventRecord(ev[0], st_));
             auto mark = [&]() { QX_CUDA(cudaEventRecord(ev[++k], st_)); };
-            if (d3) { y_fwd(psi(), g_.N); mark(); }
-            la_drift(ds_); mark();
-            if (d3) { y_inv(psi(), g_.N); mark(); }
+            if (chain) {
+                yz_drift(ds_); mark();
+            } else {
+                if (d3) { y_fwd(psi(), g_.N); mark(); }
+                la_drift(ds_); mark();
+                if (d3) { y_inv(psi(), g_.N); mark(); }
+            }
             auto a = xp();
             a.in = psi(); a.out = psi(); a.vh = vh(); a.Vout = V();
             a.pref = pref_eff(); a.rho_mean = cfg_.rho_mean; a.dt = ds_;
@@ -1167,6 +1190,8 @@ class FieldT final : public Field {
     DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, twNn_, red_, redout_, errbuf_;
     TwTables<C> tw_{};
     int* err_ = nullptr;
+    DevBuf chain_;     // drift chain: [3n] phase counters
+    int chain_n_ = 0;  // 8-column slabs of the drift chain (0: three separate passes)
     DevBuf mpsi_, mvh_, kin_, specP_, specC_, stage_;
     std::map<long, std::unique_ptr<DevBuf>> bintab_;
     std::unique_ptr<B200FFTBackend<R>> fft_;

@@ -21,6 +21,8 @@ struct Tune {
     int tma = 1;      // strided passes: 1 = persistent TMA-fed kernels, 0 = direct-load kernels
     int nbuf = 0;     // TMA ring depth (0 = as many 64 KB-class tiles as fit in ~200 KB)
     int pw = 0;       // pencils per thread of TMA passes (0 = default: 2 in FP32, 1 in FP64)
+    int chain = 0;    // FP32 3D drift's y / z / y passes: 0 three passes; 1 / 2 one slab-ordered
+                      // kernel over slabs of `chain` 8-column tiles (bit-identical, measured slower)
 };
 
 template <typename R> struct Ops {
@@ -47,6 +49,13 @@ template <typename R> struct Ops {
     // last-axis pass; returns the number of blocks (partials written for OP_KIN)
     static long la_pass(int N, const SP& s, int op, const Tune& tu, cudaStream_t st);
     static long la_blocks(int N, int X, int dim, int op, const Tune& tu);
+    // The drift chain (y forward, z forward + drift + z inverse, y inverse) of a
+    // 3D wave-function array as one kernel over x-slabs of sw 8-column tiles
+    // (FP32, N >= 16, sw = 1 or 2).  chain_slabs: slabs of the array (0: the
+    // chain does not apply); drift_chain: runs it with `cnt` (3 * slabs
+    // counters, zeroed here) on stream st.
+    static int chain_slabs(int N, int dim, int batch, int sw);
+    static void drift_chain(int N, const SP& a, int sw, unsigned* cnt, const Tune& tu, cudaStream_t st);
     // stage-major FFT twiddle table of length L from the natural-order table
     // nat[j] = exp(-2 pi i j/L) (entries beyond L - r0 are left as they are)
     static void stage_twiddles(const C* nat, int L, C* out);

@@ -11,6 +11,7 @@
 #include "qx_kernels.cuh"
 #include "qx_ops.hpp"
 #include "qx_tma.cuh"
+#include "qx_yzy.cuh"
 
 namespace qx {
 
@@ -486,6 +487,86 @@ long Ops<R>::la_pass(int N, const SP& a, int op, const Tune& tu, cudaStream_t st
         return (long)grd.x * grd.y;
     });
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// drift chain: y forward / z drift / y inverse as one slab-ordered kernel
+// ---------------------------------------------------------------------------
+
+constexpr int kChainTX = 8;  // tile columns of the chain (one slab = 8 columns)
+
+template <typename R>
+int Ops<R>::chain_slabs(int N, int dim, int batch, int sw) {
+    if (sizeof(R) != 4 || dim != 3 || N < 16 || sw < 1 || sw > 2 || N % (sw * kChainTX)) return 0;
+    bool fits = false;
+    QX_FOR_N(N, {
+        if constexpr (NN >= 16) fits = yzy_fits<NN, float, 2, kChainTX>();
+    });
+    return fits ? (batch > 0 ? batch : 1) * (N / (sw * kChainTX)) : 0;
+}
+
+template <typename R>
+void Ops<R>::drift_chain(int N, const SP& a, int sw, unsigned* cnt, const Tune& tu, cudaStream_t st) {
+    const int n_slabs = chain_slabs(N, a.dim, a.batch, sw);
+    if (!n_slabs || a.X != N || !a.tw_lo) throw std::logic_error("drift chain: not a 3D FP32 wave-function array");
+    if constexpr (sizeof(R) == 4) {
+        QX_FOR_N(N, {
+            if constexpr (NN >= 16 && yzy_fits<NN, R, 2, kChainTX>()) {
+                constexpr int PW = 2, TXF = kChainTX;
+                const TmaGeom g = tma_geom<NN, R, PW, TXF>(a.X, TXF, OP_DRIFT, tu);
+                const int nb = a.batch > 0 ? a.batch : 1;
+                YZYArgs<R> s;
+                s.tw = a.tw;
+                s.tw_lo = a.tw_lo;
+                // ring: as many tiles as fit beside the tables (at most 8)
+                const size_t tile = align1k((size_t)NN * TXF * sizeof(cx_t<R>));
+                int nbuf = (int)((227 * 1024 - yzy_smem_bytes<R>(NN, TXF, 0)) / tile);
+                if (nbuf > 8) nbuf = 8;
+                if (tu.nbuf >= 3 && tu.nbuf < nbuf) nbuf = tu.nbuf;
+                if (nbuf < 3) throw std::logic_error("drift chain: ring of fewer than 3 tiles");
+                s.sw = sw;
+                s.slabs_x = a.X / (sw * TXF);
+                s.nbuf = nbuf;
+                s.nbox = g.nbox;
+                s.box = g.box;
+                s.n_slabs = n_slabs;
+                s.n_items = 3L * n_slabs * sw * NN;
+                s.cnt = cnt;
+                s.phase_fac = a.phase_fac;
+                s.scale = a.scale;
+                s.err = a.err;
+                const CUtensorMap tmy = make_tmap<R>(a.a, a.X, NN, nb * NN, TXF, g.box, 1);
+                const CUtensorMap tmz = make_tmap<R>(a.a, a.X, NN, nb * NN, TXF, g.box, 2);
+                auto kern = k_yzy_tma<NN, R, PW, TXF>;
+                const size_t smem = yzy_smem_bytes<R>(NN, TXF, nbuf);
+                set_smem(kern, smem);
+                const int threads = yzy_block_threads<NN, R, PW, TXF>();
+                static int bps_cache[9] = {0};
+                int& bps = bps_cache[nbuf];
+                if (!bps) {
+                    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem) != cudaSuccess || bps < 1)
+                        throw std::runtime_error("drift chain: kernel does not fit an SM");
+                }
+                long grid = (long)sm_count() * bps;
+                if (grid > s.n_items) grid = s.n_items;
+                cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(unsigned) * 3 * (size_t)n_slabs, st);
+                if (e != cudaSuccess) throw std::runtime_error(std::string("drift chain: ") + cudaGetErrorString(e));
+                // cooperative: all blocks resident at once (they wait on one another's tiles)
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)grid);
+                cfg.blockDim = dim3(threads, 1, 1);
+                cfg.dynamicSmemBytes = smem;
+                cfg.stream = st;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeCooperative;
+                at[0].val.cooperative = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                e = cudaLaunchKernelEx(&cfg, kern, tmy, tmz, s);
+                if (e != cudaSuccess) throw std::runtime_error(std::string("drift chain launch: ") + cudaGetErrorString(e));
+            }
+        });
+    }
 }
 
 }  // namespace qx
