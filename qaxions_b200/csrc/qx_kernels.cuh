@@ -324,7 +324,7 @@ enum XInvMode { XI_PLAIN = 0, XI_R2C = 1 };
 // inverse c2c along x (psi^_x -> psi, times scale); optionally the density
 // source pref(|psi|^2 - rho_mean) and its r2c x transform into vh.
 template <int N, typename R, int MODE>
-__global__ void __launch_bounds__(256, 3) k_x_inv(XArgs<R> a) {
+__global__ void __launch_bounds__(256, 2) k_x_inv(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
@@ -439,7 +439,7 @@ template <int N, typename R, int FLAGS> __host__ __device__ constexpr int x_c2r_
 // its next row's vh and psi into a per-warp staging buffer with cp.async, so
 // they arrive while the forward transform and stores of the current row run.
 template <int N, typename R, int FLAGS>
-__global__ void __launch_bounds__(256, 3) k_x_c2r(XArgs<R> a) {
+__global__ void __launch_bounds__(256, 2) k_x_c2r(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
