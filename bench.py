@@ -536,7 +536,8 @@ def main():
                 "graded_roofline_26w": {
                     "bytes_per_site": ROOFLINE_BYTES_W * w,
                     "frac_of_8TBs": ROOFLINE_BYTES_W * w * S / (ms_step * 1e-3) / 8e12,
-                    "frac_of_measured": ROOFLINE_BYTES_W * w * S / (ms_step * 1e-3) / (hbm * 1e9)}}
+                    "frac_of_peak": ROOFLINE_BYTES_W * w * S / (ms_step * 1e-3) / (hbm * 1e9),
+                    "peak_kind": peak_kind}}
 
     # ---- accuracy after --accuracy-steps (FP32 vs FP64 plain form, same IC) ----
     acc = None
