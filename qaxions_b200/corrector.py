@@ -28,6 +28,7 @@ _SIGS = {
     "qx_corr_last_error": ([_vp], C.c_char_p),
     "qx_corr_nparams": ([_vp, C.POINTER(C.c_int)], C.c_int),
     "qx_corr_set_scales": ([_vp, C.c_double, C.c_double], C.c_int),
+    "qx_corr_set_tensor_path": ([_vp, C.c_int], C.c_int),
     "qx_corr_get_scales": ([_vp, _dp, _dp], C.c_int),
     "qx_corr_get_params": ([_vp, _fp], C.c_int),
     "qx_corr_set_params": ([_vp, _fp], C.c_int),
@@ -118,6 +119,10 @@ class Corrector:
         if a.size != self.nparams:
             raise ValueError(f"expected {self.nparams} parameters")
         self._c("qx_corr_set_params", a.ctypes.data_as(_fp))
+
+    def set_tensor_path(self, tc: bool):
+        """32 -> 32 convolutions on tcgen05 (True, default) or mma.sync (False)."""
+        self._c("qx_corr_set_tensor_path", int(bool(tc)))
 
     def set_scales(self, v_scale: float, tau: float):
         self._c("qx_corr_set_scales", v_scale, tau)

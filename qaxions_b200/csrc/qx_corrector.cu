@@ -191,6 +191,252 @@ __global__ void __launch_bounds__(256) k_conv(const __nv_bfloat16* __restrict__ 
         }
 }
 
+// ---------------------------------------------------------------------------
+// 32 -> 32 periodic 3^3 convolution on the 5th-generation tensor cores
+// (tcgen05.mma kind::f16: BF16 operands read from shared memory through matrix
+// descriptors, FP32 accumulators in tensor memory).
+//
+// Persistent blocks (two per SM) keep all 27 offsets' weights in shared memory
+// and walk bricks of 8 x 16 x 2 sites.  A brick is two M = 128 tiles (one per
+// z), each the GEMM [128 sites] x [K = 27 offsets x 32 channels] x [32 outputs]:
+// 54 MMAs of K = 16.  Both operands use the canonical no-swizzle K-major
+// layout, whose unit is a "core matrix" of 8 rows x 16 bytes (8 BF16 channels)
+// stored contiguously:
+//   weights  W[o]: core matrix (n-group g, channel chunk c) at ((o*4 + g)*4 + c)*128 B
+//            (K step LBO = 128 B, N step SBO = 512 B)
+//   halo     [hz][hy][c][hx][8 ch]: 16 B per (site, chunk), so the 8 sites
+//            x..x+7 of one (y, z) row of any offset are one contiguous core
+//            matrix, and an offset is just a shifted start address
+//            (K step LBO = HX*16 B, M step = next y, SBO = KC*HX*16 B)
+// One thread issues the MMAs and commits them to an mbarrier; then all eight
+// warps read the accumulators back (tcgen05.ld, warp w: tile w/4, lanes
+// 32*(w%4) ..) for the bias / GELU epilogue.  Waits are bounded; tensor memory
+// is freed on every exit path.
+// ---------------------------------------------------------------------------
+namespace tc {
+constexpr int BX = 8, BY = 16, BZ = 2;  // brick: BZ tiles of 128 sites
+constexpr int HX = BX + 2, HY = BY + 2, HZ = BZ + 2;
+constexpr int CIN = 32, COUT = 32, KC = CIN / 8;
+constexpr int HALO_BYTES = HZ * HY * KC * HX * 16;             // 46,080
+constexpr int W_BYTES = KOFF * (COUT / 8) * KC * 128;          // 55,296
+constexpr int TMEM_COLS = 64;                                  // BZ x 32 FP32 columns
+constexpr size_t SMEM = (size_t)HALO_BYTES + W_BYTES + 128;    // + alignment slack
+constexpr uint32_t LBO_A = HX * 16, SBO_A = KC * HX * 16;
+constexpr uint32_t LBO_B = 128, SBO_B = KC * 128;
+// instruction descriptor: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
+// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    // start >> 4 (bits 0-13), LBO >> 4 (16-29), SBO >> 4 (32-45), version 1
+    // (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0)
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred q;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, q;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > limit) return false;
+    }
+}
+// 32 lanes x 32 consecutive FP32 columns: thread t of the warp gets lane base + t
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+}  // namespace tc
+
+// X: [S][32] bf16; W: [27][32][40] bf16 (the packed layer weights, pitch 40);
+// outputs as k_conv.  blockDim 256; grid <= number of bricks.
+__global__ void __launch_bounds__(256, 2) k_conv_tc(const __nv_bfloat16* __restrict__ X,
+                                                    const __nv_bfloat16* __restrict__ W,
+                                                    const float* __restrict__ bias, int N, int cout, float* zf,
+                                                    __nv_bfloat16* ab, float* out2, int gelu_ab, int* err) {
+    // the brick of this kernel (the names shadow the mma.sync kernels' brick)
+    constexpr int BX = tc::BX, BY = tc::BY, BZ = tc::BZ, HX = tc::HX, HY = tc::HY, HZ = tc::HZ;
+    constexpr int CIN = tc::CIN, COUT = tc::COUT, KC = tc::KC, HALO_BYTES = tc::HALO_BYTES;
+    constexpr uint32_t TMEM_COLS = tc::TMEM_COLS;
+    using tc::commit;
+    using tc::fence_after;
+    using tc::fence_before;
+    using tc::mbar_init;
+    using tc::mbar_wait;
+    using tc::mma;
+    using tc::proxy_fence;
+    using tc::smem_addr;
+    using tc::smem_desc;
+    extern __shared__ __align__(128) unsigned char smem_tc[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ float bs[COUT];
+    __shared__ int s_fail;
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_tc) + 127) & ~(uintptr_t)127);
+    unsigned char* halo = base;
+    unsigned char* wsm = base + HALO_BYTES;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // weights -> canonical K-major core matrices; bias
+    for (int i = tid; i < KOFF * COUT * KC; i += blockDim.x) {
+        const int o = i / (COUT * KC), co = (i / KC) % COUT, c = i % KC;
+        const uint4 v = *reinterpret_cast<const uint4*>(W + ((size_t)o * COUT + co) * (CIN + 8) + c * 8);
+        *reinterpret_cast<uint4*>(wsm + ((o * (COUT / 8) + co / 8) * KC + c) * 128 + (co % 8) * 16) = v;
+    }
+    if (tid < COUT) bs[tid] = (bias && tid < cout) ? bias[tid] : 0.f;
+    if (tid == 0) {
+        s_fail = 0;
+        mbar_init(smem_addr(&mbar));
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"((uint32_t)TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    const int nbx = N / BX, nby = N / BY;
+    const long nbricks = (long)nbx * nby * (N / BZ);
+    uint32_t phase = 0;
+    for (long br = blockIdx.x; br < nbricks; br += gridDim.x) {
+        const int bxi = (int)(br % nbx), byi = (int)((br / nbx) % nby), bzi = (int)(br / ((long)nbx * nby));
+        const int x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BZ;
+        // periodic halo, 16-byte chunks: [hz][hy][c][hx], all copies in flight at once
+        for (int i = tid; i < HZ * HY * KC * HX; i += blockDim.x) {
+            const int hx = i % HX, c = (i / HX) % KC, hy = (i / (HX * KC)) % HY, hz = i / (HX * KC * HY);
+            const long gs = ((long)wrapi(z0 + hz - 1, N) * N + wrapi(y0 + hy - 1, N)) * N + wrapi(x0 + hx - 1, N);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(halo + (size_t)i * 16)),
+                         "l"(X + gs * CIN + c * 8)
+                         : "memory");
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        proxy_fence();  // shared-memory writes -> visible to the tensor cores' reads
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            const uint32_t h0 = smem_addr(halo), w0 = smem_addr(wsm);
+#pragma unroll 1
+            for (int zt = 0; zt < BZ; ++zt)
+#pragma unroll 1
+                for (int o = 0; o < KOFF; ++o) {
+                    const int hz = zt + 1 + off_dz(o), hy = 1 + off_dy(o), hx = 1 + off_dx(o);
+#pragma unroll
+                    for (int kk = 0; kk < KC / 2; ++kk) {
+                        const uint32_t a = h0 + (uint32_t)((((hz * HY + hy) * KC + 2 * kk) * HX + hx) * 16);
+                        const uint32_t b = w0 + (uint32_t)(((o * (COUT / 8)) * KC + 2 * kk) * 128);
+                        mma(tmem + (uint32_t)(zt * COUT), smem_desc(a, tc::LBO_A, tc::SBO_A),
+                            smem_desc(b, tc::LBO_B, tc::SBO_B), (o | kk) != 0);
+                    }
+                }
+            commit(smem_addr(&mbar));
+        }
+        __syncwarp();
+        if (!mbar_wait(smem_addr(&mbar), phase, 1LL << 31)) s_fail = 1;
+        phase ^= 1u;
+        fence_after();
+        // epilogue: warp w reads tile w / 4, rows 32 (w % 4) + lane (row r = site x + 8 y)
+        {
+            const int zt = warp >> 2, q = warp & 3;
+            float v[32];
+            tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(zt * COUT), v);
+            const int r = 32 * q + lane;
+            const int x = r % BX, y = r / BX;
+            const long gs = ((long)(z0 + zt) * N + (y0 + y)) * N + (x0 + x);
+#pragma unroll
+            for (int co = 0; co < COUT; ++co) v[co] += bs[co];
+            if (cout == COUT) {  // 16-byte stores of the site's 32 channels
+                if (zf) {
+#pragma unroll
+                    for (int j = 0; j < COUT / 4; ++j)
+                        reinterpret_cast<float4*>(zf + gs * COUT)[j] =
+                            make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                }
+                if (out2) {
+#pragma unroll
+                    for (int j = 0; j < COUT / 4; ++j)
+                        reinterpret_cast<float4*>(out2 + gs * COUT)[j] =
+                            make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                }
+            } else {
+#pragma unroll
+                for (int co = 0; co < COUT; ++co)
+                    if (co < cout) {
+                        if (zf) zf[gs * cout + co] = v[co];
+                        if (out2) out2[gs * cout + co] = v[co];
+                    }
+            }
+            if (ab) {
+#pragma unroll
+                for (int j = 0; j < COUT / 8; ++j) {
+                    union {
+                        __nv_bfloat162 h[4];
+                        uint4 u;
+                    } pk;
+#pragma unroll
+                    for (int q2 = 0; q2 < 4; ++q2) {
+                        const int co = 8 * j + 2 * q2;
+                        const float a0 = co < cout ? (gelu_ab ? gelu(v[co]) : v[co]) : 0.f;
+                        const float a1 = co + 1 < cout ? (gelu_ab ? gelu(v[co + 1]) : v[co + 1]) : 0.f;
+                        pk.h[q2] = __floats2bfloat162_rn(a0, a1);
+                    }
+                    reinterpret_cast<uint4*>(ab + gs * COUT)[j] = pk.u;
+                }
+            }
+        }
+        fence_before();
+        __syncthreads();  // accumulators read and halo consumed before the next brick
+        if (s_fail) break;
+    }
+    if (s_fail && tid == 0) {
+        atomicExch(err, 1);
+        mbar_wait(smem_addr(&mbar), phase ^ 1u, 1LL << 32);  // let the timed-out MMAs drain before freeing
+    }
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TMEM_COLS)
+                     : "memory");
+}
+
 // weight gradient: dW[o][ci][co] = sum_s A[s + o][ci] dZ[s][co]; db[co] = sum_s dZ[s][co]
 // A: [S][CINP] bf16 (forward input of the layer), dZ: [S][cout] FP32.
 // Persistent blocks over bricks; thread t owns 4x4 (ci, co) blocks of offsets.
@@ -464,6 +710,9 @@ class Corrector {
                                      (int)ConvSmem<32, 32>::bytes()));
         NN_CUDA(cudaFuncSetAttribute(k_conv<32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)ConvSmem<32, 8>::bytes()));
+        NN_CUDA(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM));
+        errb_.alloc(sizeof(int));
+        NN_CUDA(cudaMemset(errb_.p, 0, sizeof(int)));
         NN_CUDA(cudaFuncSetAttribute(k_wgrad<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgrad_smem(16, 32)));
         NN_CUDA(cudaFuncSetAttribute(k_wgrad<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgrad_smem(32, 32)));
     }
@@ -563,6 +812,7 @@ class Corrector {
         std::vector<double> lp(nb);
         NN_CUDA(cudaMemcpyAsync(lp.data(), lossp_.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st_));
         NN_CUDA(cudaStreamSynchronize(st_));
+        check_err();
         double loss = 0.0;
         for (double x : lp) loss += x;
         return loss / (2.0 * S);
@@ -600,9 +850,20 @@ class Corrector {
     }
     void output(float* host) {
         NN_CUDA(cudaStreamSynchronize(st_));
+        check_err();
         NN_CUDA(cudaMemcpy(host, Y_.p, sizeof(float) * 2 * S_, cudaMemcpyDeviceToHost));
     }
-    void sync() { NN_CUDA(cudaStreamSynchronize(st_)); }
+    void sync() {
+        NN_CUDA(cudaStreamSynchronize(st_));
+        check_err();
+    }
+    // 1: 32 -> 32 convolutions on the tcgen05 kernel (default), 0: all on mma.sync
+    void set_tensor_path(int tc) { use_tc_ = tc != 0; }
+    void check_err() {
+        int e = 0;
+        NN_CUDA(cudaMemcpy(&e, errb_.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) throw std::runtime_error("corrector: a tensor-core wait timed out");
+    }
 
   private:
     static size_t wgrad_smem(int cinp, int cout) { return sizeof(float) * ((size_t)HALO * cinp + (size_t)BSITES * cout); }
@@ -618,8 +879,26 @@ class Corrector {
             Z2_.alloc(sizeof(float) * 32 * S);
         }
     }
+    // 32 -> 32 layers on the tcgen05 kernel (grids N % 16 == 0), the others on mma.sync
+    bool tc_ok() const { return use_tc_ && N_ % tc::BY == 0; }
+    void conv_tc(const __nv_bfloat16* X, const __nv_bfloat16* W, const float* bias, int cout, float* zf,
+                 __nv_bfloat16* ab, float* out2, bool gelu_ab) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long nbricks = S_ / (tc::BX * tc::BY * tc::BZ);
+        const unsigned blocks = (unsigned)std::min<long>(nbricks, 2L * sms);
+        k_conv_tc<<<blocks, 256, tc::SMEM, st_>>>(X, W, bias, N_, cout, zf, ab, out2, gelu_ab ? 1 : 0,
+                                                  errb_.as<int>());
+    }
     template <int CINP, int COUTP>
     void conv(const __nv_bfloat16* X, Layer& L, float* zf, __nv_bfloat16* ab, float* out2, bool gelu_ab) {
+        if constexpr (CINP == 32 && COUTP == 32) {
+            if (tc_ok()) {
+                conv_tc(X, L.fwd.as<__nv_bfloat16>(), L.db.as<float>(), L.cout, zf, ab, out2, gelu_ab);
+                return;
+            }
+        }
         const unsigned blocks = (unsigned)(S_ / BSITES);
         k_conv<CINP, COUTP><<<blocks, 256, ConvSmem<CINP, COUTP>::bytes(), st_>>>(
             X, L.fwd.as<__nv_bfloat16>(), L.db.as<float>(), N_, L.cout, zf, ab, out2, gelu_ab ? 1 : 0);
@@ -627,6 +906,12 @@ class Corrector {
     // data gradient: input channels = the layer's outputs (padded to CINP), outputs = its inputs
     template <int CINP, int COUTP>
     void conv_bwd(const __nv_bfloat16* dZb, Layer& L, float* dA) {
+        if constexpr (CINP == 32 && COUTP == 32) {
+            if (tc_ok()) {
+                conv_tc(dZb, L.bwd.as<__nv_bfloat16>(), nullptr, L.cin, dA, nullptr, nullptr, false);
+                return;
+            }
+        }
         const unsigned blocks = (unsigned)(S_ / BSITES);
         k_conv<CINP, COUTP><<<blocks, 256, ConvSmem<CINP, COUTP>::bytes(), st_>>>(
             dZb, L.bwd.as<__nv_bfloat16>(), nullptr, N_, L.cin, dA, nullptr, nullptr, 0);
@@ -686,6 +971,8 @@ class Corrector {
     double v_scale_ = 1.0, tau_ = 1.0;
     long t_ = 0;
     DBuf X0_, A1_, A2_, Z1_, Z2_, Y_, T_, dY_, dYb_, dA_, dZ_, dZb_, lossp_, part_, fold_;
+    DBuf errb_;           // device flag: a bounded wait of the tcgen05 kernel timed out
+    bool use_tc_ = true;
 };
 
 }  // namespace nn
@@ -776,6 +1063,10 @@ const char* qx_corr_last_error(const qx_corr_t* h) {
 
 int qx_corr_nparams(qx_corr_t* h, int* n) {
     return corr_guarded(h, [&](qx::nn::Corrector& c) { *n = c.nparams(); });
+}
+
+int qx_corr_set_tensor_path(qx_corr_t* h, int tc) {
+    return corr_guarded(h, [&](qx::nn::Corrector& c) { c.set_tensor_path(tc); });
 }
 
 int qx_corr_set_scales(qx_corr_t* h, double v_scale, double tau) {

@@ -19,7 +19,9 @@ def _smooth(rng, N, amp):
     return amp * f / f.std()
 
 
-def test_corrector_gradients_match_cpu_oracle():
+@pytest.mark.parametrize("tc", [True, False])
+def test_corrector_gradients_match_cpu_oracle(tc):
+    """tc: the 32 -> 32 convolutions on tcgen05 (tensor memory) or mma.sync."""
     rng = np.random.default_rng(11)
     N = 16
     psi_c = (1.0 + _smooth(rng, N, 0.3) + 1j * _smooth(rng, N, 0.2)).astype(np.complex64).astype(np.complex128)
@@ -29,6 +31,7 @@ def test_corrector_gradients_match_cpu_oracle():
     ff = qx.Field(3, N, dtype="c64", k0="zero")
     fc.psi, fc.V, ff.psi = psi_c, V, psi_f
     corr = cr.Corrector(N, seed=3)
+    corr.set_tensor_path(tc)
     v_scale, tau = float(np.sqrt(np.mean(V ** 2))), 1e-3
     corr.set_scales(v_scale, tau)
     loss, g = corr.gradients(fc, ff)
@@ -51,6 +54,40 @@ def test_corrector_gradients_match_cpu_oracle():
     for f in (fc, ff):
         f.close()
     corr.close()
+
+
+@pytest.mark.parametrize("N", [32, 96])
+def test_tensor_paths_agree(N):
+    """The tcgen05 kernel (8 x 16 x 2 bricks, tensor-memory accumulators) and the
+    mma.sync kernel compute the same 32 -> 32 convolutions: outputs and all
+    parameter gradients agree to FP32 summation order and the BF16 rounding of
+    the activations that follow (two calls each, so a stale state would show)."""
+    rng = np.random.default_rng(5 + N)
+    psi_c = (1.0 + _smooth(rng, N, 0.3) + 1j * _smooth(rng, N, 0.2)).astype(np.complex64).astype(np.complex128)
+    V = _smooth(rng, N, 2.0).astype(np.float32).astype(np.float64)
+    psi_f = (psi_c + 1e-3 * (_smooth(rng, N, 1.0) + 1j * _smooth(rng, N, 1.0))).astype(np.complex64).astype(np.complex128)
+    fc = qx.Field(3, N, dtype="c64", k0="zero")
+    ff = qx.Field(3, N, dtype="c64", k0="zero")
+    fc.psi, fc.V, ff.psi = psi_c, V, psi_f
+    res = {}
+    for tc in (True, False):
+        corr = cr.Corrector(N, seed=9)
+        corr.set_tensor_path(tc)
+        corr.set_scales(float(np.sqrt(np.mean(V ** 2))), 1e-3)
+        out = []
+        for _ in range(2):
+            loss, g = corr.gradients(fc, ff)
+            out.append((loss, g.astype(np.float64), corr.output().astype(np.float64)))
+        res[tc] = out
+        corr.close()
+    for (l1, g1, y1), (l0, g0, y0) in zip(res[True], res[False]):
+        assert np.isfinite(g1).all() and np.isfinite(y1).all()
+        assert abs(l1 - l0) <= 1e-4 * l0, (l1, l0)
+        assert O.rel_l2(y1, y0) <= 1e-3
+        assert O.rel_l2(g1, g0) <= 1e-3
+    assert np.array_equal(res[True][0][1], res[True][1][1])  # deterministic
+    for f in (fc, ff):
+        f.close()
 
 
 def test_training_reduces_the_coarse_step_error():
