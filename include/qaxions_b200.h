@@ -214,9 +214,10 @@ int qx_corr_destroy(qx_corr_t *h);
 const char *qx_corr_last_error(const qx_corr_t *h);
 int qx_corr_nparams(qx_corr_t *h, int *n);
 int qx_corr_set_scales(qx_corr_t *h, double v_scale, double tau);
-/* Tensor path of the 32 -> 32 convolutions (forward and data gradient of the
- * middle layer): 1 (default) tcgen05.mma with tensor-memory accumulators, for
- * grids with N % 16 == 0; 0 the mma.sync kernel that the other layers use. */
+/* Tensor path of the convolutions with 32 outputs (forward of the first and
+ * middle layers, data gradients of the middle and last layers): 1 (default)
+ * tcgen05.mma with tensor-memory accumulators, for grids with N % 16 == 0; 0
+ * the mma.sync kernel that the last layer's forward always uses. */
 int qx_corr_set_tensor_path(qx_corr_t *h, int tc);
 int qx_corr_get_scales(qx_corr_t *h, double *v_scale, double *tau);
 int qx_corr_get_params(qx_corr_t *h, float *params);

@@ -192,18 +192,21 @@ __global__ void __launch_bounds__(256) k_conv(const __nv_bfloat16* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// 32 -> 32 periodic 3^3 convolution on the 5th-generation tensor cores
-// (tcgen05.mma kind::f16: BF16 operands read from shared memory through matrix
-// descriptors, FP32 accumulators in tensor memory).
+// CIN -> 32 periodic 3^3 convolutions (CIN = 16 or 32) on the 5th-generation
+// tensor cores (tcgen05.mma kind::f16: BF16 operands read from shared memory
+// through matrix descriptors, FP32 accumulators in tensor memory).
 //
 // Persistent blocks (two per SM) keep all 27 offsets' weights in shared memory
 // and walk bricks of 8 x 16 x 2 sites.  A brick is two M = 128 tiles (one per
-// z), each the GEMM [128 sites] x [K = 27 offsets x 32 channels] x [32 outputs]:
-// 54 MMAs of K = 16.  Both operands use the canonical no-swizzle K-major
+// z), each the GEMM [128 sites] x [K = 27 offsets x CIN channels] x [32
+// outputs]: 27 CIN / 16 MMAs of K = 16.  (A one-block-per-SM version with a
+// dedicated MMA warp, triple-buffered halos and double-buffered accumulators
+// measured slower: with N = 32 the two independent blocks overlap each other's
+// halo loads and epilogues better.)  Both operands use the canonical no-swizzle K-major
 // layout, whose unit is a "core matrix" of 8 rows x 16 bytes (8 BF16 channels)
 // stored contiguously:
-//   weights  W[o]: core matrix (n-group g, channel chunk c) at ((o*4 + g)*4 + c)*128 B
-//            (K step LBO = 128 B, N step SBO = 512 B)
+//   weights  W[o]: core matrix (n-group g, channel chunk c) at ((o*4 + g)*KC + c)*128 B
+//            (K step LBO = 128 B, N step SBO = KC*128 B; KC = CIN / 8)
 //   halo     [hz][hy][c][hx][8 ch]: 16 B per (site, chunk), so the 8 sites
 //            x..x+7 of one (y, z) row of any offset are one contiguous core
 //            matrix, and an offset is just a shifted start address
@@ -216,13 +219,16 @@ __global__ void __launch_bounds__(256) k_conv(const __nv_bfloat16* __restrict__ 
 namespace tc {
 constexpr int BX = 8, BY = 16, BZ = 2;  // brick: BZ tiles of 128 sites
 constexpr int HX = BX + 2, HY = BY + 2, HZ = BZ + 2;
-constexpr int CIN = 32, COUT = 32, KC = CIN / 8;
-constexpr int HALO_BYTES = HZ * HY * KC * HX * 16;             // 46,080
-constexpr int W_BYTES = KOFF * (COUT / 8) * KC * 128;          // 55,296
-constexpr int TMEM_COLS = 64;                                  // BZ x 32 FP32 columns
-constexpr size_t SMEM = (size_t)HALO_BYTES + W_BYTES + 128;    // + alignment slack
-constexpr uint32_t LBO_A = HX * 16, SBO_A = KC * HX * 16;
-constexpr uint32_t LBO_B = 128, SBO_B = KC * 128;
+constexpr int COUT = 32;
+constexpr int TMEM_COLS = 64;  // BZ x 32 FP32 columns
+template <int CIN> struct Geo {
+    static constexpr int KC = CIN / 8;                                 // 16-byte channel chunks
+    static constexpr int HALO_BYTES = HZ * HY * KC * HX * 16;          // 46,080 for CIN = 32
+    static constexpr int W_BYTES = KOFF * (COUT / 8) * KC * 128;       // 55,296 for CIN = 32
+    static constexpr size_t SMEM = (size_t)HALO_BYTES + W_BYTES + 128;  // + alignment slack
+    static constexpr uint32_t LBO_A = HX * 16, SBO_A = KC * HX * 16;
+    static constexpr uint32_t LBO_B = 128, SBO_B = KC * 128;
+};
 // instruction descriptor: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
 // both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(COUT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
@@ -284,15 +290,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 }
 }  // namespace tc
 
-// X: [S][32] bf16; W: [27][32][40] bf16 (the packed layer weights, pitch 40);
+// X: [S][CIN] bf16; W: [27][32][CIN + 8] bf16 (the packed layer weights);
 // outputs as k_conv.  blockDim 256; grid <= number of bricks.
+template <int CIN>
 __global__ void __launch_bounds__(256, 2) k_conv_tc(const __nv_bfloat16* __restrict__ X,
                                                     const __nv_bfloat16* __restrict__ W,
                                                     const float* __restrict__ bias, int N, int cout, float* zf,
                                                     __nv_bfloat16* ab, float* out2, int gelu_ab, int* err) {
     // the brick of this kernel (the names shadow the mma.sync kernels' brick)
     constexpr int BX = tc::BX, BY = tc::BY, BZ = tc::BZ, HX = tc::HX, HY = tc::HY, HZ = tc::HZ;
-    constexpr int CIN = tc::CIN, COUT = tc::COUT, KC = tc::KC, HALO_BYTES = tc::HALO_BYTES;
+    using G = tc::Geo<CIN>;
+    constexpr int COUT = tc::COUT, KC = G::KC, HALO_BYTES = G::HALO_BYTES;
     constexpr uint32_t TMEM_COLS = tc::TMEM_COLS;
     using tc::commit;
     using tc::fence_after;
@@ -364,8 +372,8 @@ __global__ void __launch_bounds__(256, 2) k_conv_tc(const __nv_bfloat16* __restr
                     for (int kk = 0; kk < KC / 2; ++kk) {
                         const uint32_t a = h0 + (uint32_t)((((hz * HY + hy) * KC + 2 * kk) * HX + hx) * 16);
                         const uint32_t b = w0 + (uint32_t)(((o * (COUT / 8)) * KC + 2 * kk) * 128);
-                        mma(tmem + (uint32_t)(zt * COUT), smem_desc(a, tc::LBO_A, tc::SBO_A),
-                            smem_desc(b, tc::LBO_B, tc::SBO_B), (o | kk) != 0);
+                        mma(tmem + (uint32_t)(zt * COUT), smem_desc(a, G::LBO_A, G::SBO_A),
+                            smem_desc(b, G::LBO_B, G::SBO_B), (o | kk) != 0);
                     }
                 }
             commit(smem_addr(&mbar));
@@ -710,7 +718,8 @@ class Corrector {
                                      (int)ConvSmem<32, 32>::bytes()));
         NN_CUDA(cudaFuncSetAttribute(k_conv<32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)ConvSmem<32, 8>::bytes()));
-        NN_CUDA(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM));
+        NN_CUDA(cudaFuncSetAttribute(k_conv_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::Geo<32>::SMEM));
+        NN_CUDA(cudaFuncSetAttribute(k_conv_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::Geo<16>::SMEM));
         errb_.alloc(sizeof(int));
         NN_CUDA(cudaMemset(errb_.p, 0, sizeof(int)));
         NN_CUDA(cudaFuncSetAttribute(k_wgrad<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgrad_smem(16, 32)));
@@ -879,23 +888,26 @@ class Corrector {
             Z2_.alloc(sizeof(float) * 32 * S);
         }
     }
-    // 32 -> 32 layers on the tcgen05 kernel (grids N % 16 == 0), the others on mma.sync
+    // CIN -> 32 layers on the tcgen05 kernel (grids N % 16 == 0), the others on mma.sync
     bool tc_ok() const { return use_tc_ && N_ % tc::BY == 0; }
+    template <int CIN>
     void conv_tc(const __nv_bfloat16* X, const __nv_bfloat16* W, const float* bias, int cout, float* zf,
                  __nv_bfloat16* ab, float* out2, bool gelu_ab) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        // two blocks per SM (the kernel's launch bounds; the shared-memory carve-out is
+        // set at launch), so one block's MMAs overlap the other's halo loads and epilogue
         const long nbricks = S_ / (tc::BX * tc::BY * tc::BZ);
         const unsigned blocks = (unsigned)std::min<long>(nbricks, 2L * sms);
-        k_conv_tc<<<blocks, 256, tc::SMEM, st_>>>(X, W, bias, N_, cout, zf, ab, out2, gelu_ab ? 1 : 0,
-                                                  errb_.as<int>());
+        k_conv_tc<CIN><<<blocks, 256, tc::Geo<CIN>::SMEM, st_>>>(X, W, bias, N_, cout, zf, ab, out2, gelu_ab ? 1 : 0,
+                                                                 errb_.as<int>());
     }
     template <int CINP, int COUTP>
     void conv(const __nv_bfloat16* X, Layer& L, float* zf, __nv_bfloat16* ab, float* out2, bool gelu_ab) {
-        if constexpr (CINP == 32 && COUTP == 32) {
+        if constexpr ((CINP == 32 || CINP == 16) && COUTP == 32) {
             if (tc_ok()) {
-                conv_tc(X, L.fwd.as<__nv_bfloat16>(), L.db.as<float>(), L.cout, zf, ab, out2, gelu_ab);
+                conv_tc<CINP>(X, L.fwd.as<__nv_bfloat16>(), L.db.as<float>(), L.cout, zf, ab, out2, gelu_ab);
                 return;
             }
         }
@@ -906,9 +918,9 @@ class Corrector {
     // data gradient: input channels = the layer's outputs (padded to CINP), outputs = its inputs
     template <int CINP, int COUTP>
     void conv_bwd(const __nv_bfloat16* dZb, Layer& L, float* dA) {
-        if constexpr (CINP == 32 && COUTP == 32) {
+        if constexpr ((CINP == 32 || CINP == 16) && COUTP == 32) {
             if (tc_ok()) {
-                conv_tc(dZb, L.bwd.as<__nv_bfloat16>(), nullptr, L.cin, dA, nullptr, nullptr, false);
+                conv_tc<CINP>(dZb, L.bwd.as<__nv_bfloat16>(), nullptr, L.cin, dA, nullptr, nullptr, false);
                 return;
             }
         }
