@@ -184,11 +184,46 @@ def cpu_baseline(psi0, dt, budget_s=20.0):
         f.loop_body(1)
         t += time.perf_counter() - t0
         n += 1
+    cal = fft_calibration(f, cores)
     f.close()
     S = N_GRID ** DIM
-    return {"value": S * n / t, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{n} KDK loop-body step(s) of the 512^3 state (complex128, reference loops + project FFTW shim)",
-            "s_per_step": t / n}
+    out = {"value": S * n / t, "unit": UNIT, "cores": cores, "kind": "reference",
+           "sample": f"{n} KDK loop-body step(s) of the 512^3 state (complex128, reference loops + project FFTW shim)",
+           "s_per_step": t / n, "fft_calibration": cal}
+    if cal and cal.get("shim_over_scipy"):
+        # a loop-body step runs 2 c2c + 1 r2c + 1 c2r (about 3 c2c of work): the
+        # step time with an FFT as fast as scipy's instead of the shim's
+        t_fast = max(t / n - 3.0 * (cal["shim_c2c_s"] - cal["scipy_c2c_s"]), 1e-9)
+        out["value_if_fft_as_fast_as_scipy"] = S / t_fast
+    return out
+
+
+def fft_calibration(ref_field, cores):
+    """How fast the project FFTW shim (the reference build's FFT) is: one
+    forward 512^3 complex128 c2c through the reference's FFT plugin, beside
+    scipy.fft.fftn (pocketfft, `cores` worker threads) on the same array."""
+    try:
+        import ctypes as C
+
+        import scipy.fft as sf
+
+        from oracle import ref_lib as R
+    except ImportError:
+        return None
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal((N_GRID,) * DIM) + 1j * rng.standard_normal((N_GRID,) * DIM)).astype(np.complex128)
+    y = x.copy()
+    t0 = time.perf_counter()
+    R.lib().ref_fft_forward_c2c(ref_field.h, y.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    t_shim = time.perf_counter() - t0
+    sf.fftn(x[:64, :64, :64], workers=cores)  # warm the plan cache
+    t0 = time.perf_counter()
+    z = sf.fftn(x, workers=cores, overwrite_x=False)
+    t_sc = time.perf_counter() - t0
+    err = float(np.linalg.norm(z - y) / np.linalg.norm(z))
+    del x, y, z
+    return {"grid": N_GRID, "shim_c2c_s": t_shim, "scipy_c2c_s": t_sc, "shim_over_scipy": t_shim / t_sc,
+            "relL2_shim_vs_scipy": err, "workers": cores}
 
 
 def run_reference_arm(args, world, rank):
@@ -277,12 +312,13 @@ def run_ensemble(args, world, rank, local):
     import qaxions_b200 as qx
     qx.set_device(local)
     groups, mine = qx.shard_groups(ENSEMBLE, world, rank)
+    seeds = [1234 + b for b in mine]  # every box keeps its global seed on any rank
     dt = 0.2 / 128**2
     K, W = args.steps, args.warmup
     res = {}
     for dtype in ("c64", "c128"):
         e = qx.Ensemble(groups, dtype=dtype, dt=dt)
-        e.ic_config(qx.IC_GRF, seed_base=1234)
+        e.ic_config(qx.IC_GRF, seeds=seeds)
         e.step(W)
         barrier_sync(world)
         ms = e.time_steps(K)
@@ -298,8 +334,8 @@ def run_ensemble(args, world, rank, local):
     if rank == 0 and args.accuracy_steps > 0:
         a = qx.Ensemble(groups, dtype="c128", dt=dt)
         b = qx.Ensemble(groups, dtype="c64", dt=dt)
-        a.ic_config(qx.IC_GRF, seed_base=1234)
-        b.ic_config(qx.IC_GRF, seed_base=1234)
+        a.ic_config(qx.IC_GRF, seeds=seeds)
+        b.ic_config(qx.IC_GRF, seeds=seeds)
         a.step(args.accuracy_steps)
         b.step(args.accuracy_steps)
         errs = [float(np.linalg.norm(b.psi(i) - a.psi(i)) / np.linalg.norm(a.psi(i))) for i in range(a.nboxes)]

@@ -106,6 +106,46 @@ int qx_mass_energy(qx_field_t *h, double *M, double *E, double *K, double *W);
  * (N/2+1 for QX_SPEC_REFERENCE, nbins ignored). */
 int qx_spectrum(qx_field_t *h, int source, int mode, int nbins, double *k, double *P, long long *count);
 
+/* ---- measurements (src/meas.h, src/meas.cxx:13-63, src/enum.h:39-47) ----
+ * MeasureType bits of the reference, and two of this library's own. */
+#define QX_MEAS_NONE 0u
+#define QX_MEAS_SPECTRUM (1u << 0)   /* spec_NNNN.txt: reference shells of |psi|^2 */
+#define QX_MEAS_RHO_MAX (1u << 1)    /* rhomax (taken whenever the mask is not NONE) */
+#define QX_MEAS_RHO_SLICE (1u << 2)  /* enumerated by the reference; its measure() ignores it */
+#define QX_MEAS_RHO_GRID (1u << 3)   /* field_NNNN.rho (raw FP64 rho) + field_NNNN.json Header */
+#define QX_MEAS_PSI_GRID (1u << 4)   /* enumerated by the reference; its measure() ignores it */
+#define QX_MEAS_ENERGY (1u << 8)     /* mass and energy (no reference counterpart) */
+#define QX_MEAS_CLOBBER_V (1u << 9)  /* leave V = |psi|^2 afterwards, as the reference's
+                                        computeEnergy does (src/field.cxx:205-211) */
+/* one measurement: the values measure()/printStatus report (src/utils.cxx:64-85)
+ * plus this library's diagnostics; mass/energy/kinetic/potential are NaN
+ * unless QX_MEAS_ENERGY */
+typedef struct {
+    int number;        /* measurement number, 0 = before the loop */
+    int step;          /* Field::curr() */
+    double time;       /* Field::time() */
+    double a;          /* Field::a() */
+    double rhomax;     /* max |psi|^2 / mean |psi|^2 (computeEnergy) */
+    double vmax;       /* max |V| of the potential of this psi */
+    double mass, energy, kinetic, potential;
+} qx_meas_t;
+/* generateMeasList (src/utils.cxx:8-28): the loop indices after whose
+ * drift_update main() measures; *n_out = number written (<= max_out) */
+int qx_meas_list(long long nsteps, long long nmeas, long long *out, int max_out, int *n_out);
+/* measure(Field&, Params&, measNumber, ...) (src/meas.cxx:13-63) of the current
+ * state.  Unlike the reference it leaves V alone unless mask has
+ * QX_MEAS_CLOBBER_V.  Files (spec_NNNN.txt, field_NNNN.*, measurements.jsonl)
+ * go to directory `dir` when it is not NULL.  rec may be NULL. */
+int qx_measure(qx_field_t *h, unsigned mask, int number, const char *dir, qx_meas_t *rec);
+/* The time loop of main() (src/main.cxx:60-85) with its measurements:
+ * measure(0), updatePotential, half_kick, then for every loop index idx
+ * drift_update, measure(k) if idx is the k-th entry of
+ * qx_meas_list(nsteps, nmeas), full_kick but the last; final half_kick.
+ * Unmeasured loop bodies are the fused, graph-replayed passes of qx_step.
+ * recs holds max_recs records (nmeas + 1 suffice); *n_out = records taken. */
+int qx_run(qx_field_t *h, int nsteps, int nmeas, unsigned mask, const char *dir, qx_meas_t *recs, int max_recs,
+           int *n_out);
+
 /* FFTBackend::forward_c2c / backward_c2c / forward_r2c / backward_c2r
  * (src/fft/fft.h:14-17) on host buffers; sign -1 forward, +1 backward;
  * r2c/c2r halves use FFTW's [..][N/2+1] layout; all unnormalised. */
@@ -162,6 +202,13 @@ int qx_psi_changed(qx_field_t *h);
  * and every step ds = 0.00025 / a, a *= 1 + 1.27^2 sqrt(1 + a) ds
  * (src/field.cxx:70-90, 349-361).  MRE steps run without the loop-body graph. */
 int qx_set_cosmology(qx_field_t *h, int cosmo, double ai);
+/* cosmology state Field::a_ / ds_ (src/field.h:80-82): mode (0 STATIC, 1
+ * MRE), scale factor and current time step */
+int qx_get_cosmology(qx_field_t *h, int *cosmo, double *a, double *ds);
+/* restore a and ds of a checkpoint after qx_set_cosmology (which starts the
+ * cosmology afresh); the reference's checkpoint header stores a
+ * (IO::writeConf, src/io/io.cxx:362-367) but its reader does not restore it */
+int qx_restore_cosmology(qx_field_t *h, double a, double ds);
 /* set the step counter and time (restoring a checkpoint) */
 int qx_set_clock(qx_field_t *h, int step, double time);
 /* psi *= factor (real) */
@@ -189,6 +236,10 @@ int qx_ens_box_n(qx_ens_t *h, int box, int *N);
 /* initial conditions as qx_ic_config, box b seeded with seed_base + b */
 int qx_ens_ic_config(qx_ens_t *h, int kind, unsigned long long seed_base, int n_sol, double rc_lo,
                      double rc_hi, double sigma, double kc_factor, double clip, double rho0);
+/* the same with one seed per box (nboxes values): an ensemble sharded over
+ * several processes seeds each local box by its global box index */
+int qx_ens_ic_config_seeds(qx_ens_t *h, int kind, const unsigned long long *seeds, int n_sol, double rc_lo,
+                           double rc_hi, double sigma, double kc_factor, double clip, double rho0);
 int qx_ens_set_psi(qx_ens_t *h, int box, const double *psi);
 int qx_ens_get_psi(qx_ens_t *h, int box, double *psi);
 /* nsteps merged KDK steps of every box (returns when all are done) */
@@ -236,19 +287,21 @@ int qx_corr_apply(qx_corr_t *h, void *psi, const void *V, void *stream);
 int qx_corr_output(qx_corr_t *h, float *out);
 
 /* Allocation-free density statistics of a psi array in the CALLER's device
- * memory (no counterpart in the reference).  For callers that may not allocate
- * device memory while they run: an application whose own pool or caching
- * allocator owns the device memory, a time loop that cannot take the implicit
- * synchronisation of cudaMalloc/cudaFree, a fixed memory budget.  Computes
- * out[0] = sum |psi|^2, out[1] = max |psi|^2, out[2] = out[1] / (out[0]/sites)
- * (the rhomax of Field::computeEnergy, src/field.cxx:216-226) into `out`, 3
- * doubles of device memory, asynchronously on `stream` (a cudaStream_t, NULL
- * for the default stream).  psi: `sites` complex values (dtype QX_C128 double2
- * or QX_C64 float2) on the current device.  Scratch is a fixed per-device array
- * inside the library sized for at most QX_NOALLOC_MAX_SITES sites; larger
- * sizes are rejected.  The first call on a device looks up that array's device
- * address -- make it before any stream capture.  Calls that overlap on the GPU
- * share the scratch and race.  Errors: qx_noalloc_last_error(). */
+ * memory.  This entry point has no counterpart in the reference.  It is for
+ * callers that may not allocate device memory while they run: an application
+ * whose own pool or caching allocator owns the device memory, a time loop that
+ * cannot take the implicit synchronisation of cudaMalloc/cudaFree, a fixed
+ * memory budget.  Computes out[0] = sum |psi|^2, out[1] = max |psi|^2 and
+ * out[2] = out[1] / (out[0]/sites) (max density over mean density; a NaN in
+ * psi gives NaN) into `out`, 3 doubles of device memory, asynchronously on
+ * `stream` (a cudaStream_t, NULL for the default stream).  psi: `sites`
+ * complex values (dtype QX_C128 double2 or QX_C64 float2) inside one device
+ * allocation of the current device; `out` likewise.  Scratch is a fixed
+ * per-device array inside the library sized for at most QX_NOALLOC_MAX_SITES
+ * sites; larger sizes are rejected.  The first call on a device looks up that
+ * array's device address -- make it before any stream capture.  Calls that
+ * overlap on the GPU share the scratch and race.
+ * Errors: qx_noalloc_last_error(). */
 #define QX_NOALLOC_MAX_SITES 134217728LL /* 512^3 */
 int qx_rho_stats_noalloc(const void *psi, long long sites, int dtype, double *out, void *stream);
 const char *qx_noalloc_last_error(void);

@@ -55,6 +55,8 @@ def lib():
             "ref_run": ([vp, i], None),
             "ref_loop_body": ([vp, i], None),
             "ref_spectrum": ([vp, dp, ip, dp], None),
+            "ref_meas_list": ([C.c_longlong, C.c_longlong, C.POINTER(C.c_longlong)], i),
+            "ref_run_measured": ([vp, i, i, i, i, dp, ip, dp, dp, ip], i),
             "ref_fft_forward_c2c": ([vp, dp], None),
             "ref_fft_backward_c2c": ([vp, dp], None),
             "ref_fft_forward_r2c": ([vp, dp, dp], None),
@@ -66,6 +68,13 @@ def lib():
             f.restype = res
         _lib = L
     return _lib
+
+
+def meas_list(nsteps: int, nmeas: int):
+    """The reference's own generateMeasList (src/utils.cxx:8-28)."""
+    out = (C.c_longlong * max(nmeas, 1))()
+    n = lib().ref_meas_list(nsteps, nmeas, out)
+    return [int(out[k]) for k in range(n)]
 
 
 def _dp(a: np.ndarray):
@@ -126,6 +135,20 @@ class RefField:
         c = np.empty(nb, np.int32)
         lib().ref_spectrum(self.h, _dp(P), c.ctypes.data_as(C.POINTER(C.c_int)), _dp(k))
         return k, P, c.astype(np.int64)
+
+    def run_measured(self, nsteps: int, nmeas: int, clobber: bool, spectrum: bool):
+        """The reference's main loop with measurements (ref_run_measured):
+        (rhomax, curr, time, P[m, b], counts[m, b]) per measurement."""
+        nb = self.N // 2 + 1
+        cap = nmeas + 1
+        rm, tm = np.zeros(cap), np.zeros(cap)
+        cu = np.zeros(cap, np.int32)
+        P = np.zeros((cap, nb))
+        cnt = np.zeros((cap, nb), np.int32)
+        m = lib().ref_run_measured(self.h, nsteps, nmeas, int(clobber), int(spectrum), _dp(rm),
+                                   cu.ctypes.data_as(C.POINTER(C.c_int)), _dp(tm), _dp(P),
+                                   cnt.ctypes.data_as(C.POINTER(C.c_int)))
+        return rm[:m], cu[:m], tm[:m], P[:m], cnt[:m].astype(np.int64)
 
     def __getattr__(self, name):
         f = getattr(lib(), "ref_" + name)

@@ -20,6 +20,7 @@
 #include "parse.h"
 #include "profiler.h"
 #include "spectrum/spectrum.h"
+#include "utils.h"
 
 // src/meas.cxx:8-11 needs HDF5 for the rest of its file; this one cast is all
 // src/parse.cxx uses from it.
@@ -134,6 +135,63 @@ void ref_run(void* p, int nsteps) {
         if (idx != nsteps - 1) f.full_kick();
     }
     f.half_kick();
+}
+
+// generateMeasList (src/utils.cxx:8-28), the reference's own function; out
+// holds at least nmeas entries; returns the number written.
+int ref_meas_list(long long nsteps, long long nmeas, long long* out) {
+    const auto v = generateMeasList((size_t)nsteps, (size_t)nmeas);
+    for (size_t i = 0; i < v.size(); ++i) out[i] = (long long)v[i];
+    return (int)v.size();
+}
+
+// src/main.cxx:60-85 with measurements.  measure() (src/meas.cxx:13-63) needs
+// HDF5 for its file output, so its dispatch is spelled out here with what it
+// computes: computeEnergy (rhomax; V <- rho) and, for the spectrum bit, the
+// Spectrum of that V (src/meas.cxx:30-45).  clobber = 1 keeps the reference's
+// behaviour (the kick after a measurement uses V = rho); clobber = 0 measures
+// on a copy of V.  Per measurement m (0 .. returned count - 1): rhomax[m],
+// curr[m], time[m], and (spectrum != 0) P[m*nb + b], counts[m*nb + b] with
+// nb = N/2 + 1.
+int ref_run_measured(void* p, int nsteps, int nmeas, int clobber, int spectrum, double* rhomax, int* curr,
+                     double* time, double* P, int* counts) {
+    Field& f = F(p);
+    const auto mlist = generateMeasList((size_t)nsteps, (size_t)nmeas);
+    int m = 0;
+    std::vector<double> vsave;
+    auto meas = [&]() {
+        if (!clobber) vsave.assign(f.V(), f.V() + f.sites());
+        f.computeEnergy();
+        rhomax[m] = f.rhomax();
+        curr[m] = f.curr();
+        time[m] = f.time();
+        if (spectrum) {
+            Spectrum s(f);
+            s.compute();
+            const auto& pk = s.Pk();
+            const auto& c = s.counts();
+            for (size_t b = 0; b < pk.size(); ++b) {
+                P[(size_t)m * pk.size() + b] = pk[b];
+                counts[(size_t)m * pk.size() + b] = c[b];
+            }
+        }
+        if (!clobber) std::memcpy(f.V(), vsave.data(), sizeof(double) * vsave.size());
+        ++m;
+    };
+    meas();
+    f.updatePotential();
+    f.half_kick();
+    size_t next = 0;
+    for (int idx = 0; idx < nsteps; ++idx) {
+        f.drift_update();
+        if (next < mlist.size() && (size_t)idx == mlist[next]) {
+            ++next;
+            meas();
+        }
+        if (idx != nsteps - 1) f.full_kick();
+    }
+    f.half_kick();
+    return m;
 }
 
 // Partial loop used to time a bounded CPU sample: `nsteps` iterations of the

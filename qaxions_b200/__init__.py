@@ -38,6 +38,21 @@ _ip = C.POINTER(C.c_int)
 _llp = C.POINTER(C.c_longlong)
 _fp = C.POINTER(C.c_float)
 
+# MeasureType bits (src/enum.h:39-47) and this library's own
+MEAS_NONE, MEAS_SPECTRUM, MEAS_RHO_MAX, MEAS_RHO_SLICE, MEAS_RHO_GRID, MEAS_PSI_GRID = 0, 1, 2, 4, 8, 16
+MEAS_ENERGY, MEAS_CLOBBER_V = 1 << 8, 1 << 9
+
+
+class MeasRecord(C.Structure):
+    """qx_meas_t: one measurement of measure() (src/meas.cxx:13-63)."""
+    _fields_ = [("number", C.c_int), ("step", C.c_int), ("time", C.c_double), ("a", C.c_double),
+                ("rhomax", C.c_double), ("vmax", C.c_double), ("mass", C.c_double), ("energy", C.c_double),
+                ("kinetic", C.c_double), ("potential", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _SIGS = {
     "qx_version": ([], _i),
     "qx_last_error": ([_vp], C.c_char_p),
@@ -66,6 +81,9 @@ _SIGS = {
     "qx_rho_stats": ([_vp, _dp, _dp], _i),
     "qx_mass_energy": ([_vp, _dp, _dp, _dp, _dp], _i),
     "qx_spectrum": ([_vp, _i, _i, _i, _dp, _dp, _llp], _i),
+    "qx_meas_list": ([C.c_longlong, C.c_longlong, _llp, _i, _ip], _i),
+    "qx_measure": ([_vp, C.c_uint, _i, C.c_char_p, C.POINTER(MeasRecord)], _i),
+    "qx_run": ([_vp, _i, _i, C.c_uint, C.c_char_p, C.POINTER(MeasRecord), _i, _ip], _i),
     "qx_fft_c2c": ([_vp, _dp, _i], _i),
     "qx_fft_r2c": ([_vp, _dp, _dp], _i),
     "qx_fft_c2r": ([_vp, _dp, _dp], _i),
@@ -81,12 +99,15 @@ _SIGS = {
     "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
     "qx_set_clock": ([_vp, _i, _d], _i),
     "qx_set_cosmology": ([_vp, _i, _d], _i),
+    "qx_get_cosmology": ([_vp, _ip, _dp, _dp], _i),
+    "qx_restore_cosmology": ([_vp, _d, _d], _i),
     "qx_ens_create": ([_i, _ip, _ip, _i, _d, _d, _i, _d, C.POINTER(_vp)], _i),
     "qx_ens_destroy": ([_vp], _i),
     "qx_ens_last_error": ([_vp], C.c_char_p),
     "qx_ens_size": ([_vp, _ip, _llp], _i),
     "qx_ens_box_n": ([_vp, _i, _ip], _i),
     "qx_ens_ic_config": ([_vp, _i, C.c_ulonglong, _i, _d, _d, _d, _d, _d, _d], _i),
+    "qx_ens_ic_config_seeds": ([_vp, _i, C.POINTER(C.c_ulonglong), _i, _d, _d, _d, _d, _d, _d], _i),
     "qx_ens_set_psi": ([_vp, _i, _dp], _i),
     "qx_ens_get_psi": ([_vp, _i, _dp], _i),
     "qx_ens_step": ([_vp, _i], _i),
@@ -124,6 +145,15 @@ def _check(status: int, h=None):
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_dp)
+
+
+def meas_list(nsteps: int, nmeas: int):
+    """generateMeasList (src/utils.cxx:8-28): the loop indices after whose
+    drift_update the time loop measures."""
+    out = (C.c_longlong * max(int(nmeas), 1))()
+    n = C.c_int()
+    _check(_lib.qx_meas_list(int(nsteps), int(nmeas), out, max(int(nmeas), 1), C.byref(n)))
+    return [int(out[i]) for i in range(n.value)]
 
 
 def set_device(device: int):
@@ -317,6 +347,25 @@ class Field:
         self._c("qx_spectrum", source, mode, nbins, _ptr(k), _ptr(P), cnt.ctypes.data_as(_llp))
         return k, P, cnt
 
+    def measure(self, mask: int = MEAS_RHO_MAX, number: int = 0, directory: str | None = None) -> dict:
+        """measure() (src/meas.cxx:13-63) of the current state: rhomax and Vmax,
+        the spectrum file (MEAS_SPECTRUM) and density grid (MEAS_RHO_GRID) in
+        `directory`, mass and energy (MEAS_ENERGY).  V is left alone unless
+        MEAS_CLOBBER_V."""
+        r = MeasRecord()
+        self._c("qx_measure", mask, number, directory.encode() if directory else None, C.byref(r))
+        return r.as_dict()
+
+    def run(self, nsteps: int, nmeas: int, mask: int = MEAS_RHO_MAX, directory: str | None = None):
+        """The time loop of main() (src/main.cxx:60-85) with measure(0) and one
+        measurement after each scheduled drift_update (meas_list); returns the
+        records (dicts), also written to `directory`/measurements.jsonl."""
+        recs = (MeasRecord * (nmeas + 1))()
+        n = C.c_int()
+        self._c("qx_run", nsteps, nmeas, mask, directory.encode() if directory else None, recs, nmeas + 1,
+                C.byref(n))
+        return [recs[i].as_dict() for i in range(n.value)]
+
     # -- FFT plugin on host buffers --
     def fft_c2c(self, data: np.ndarray, sign: int) -> np.ndarray:
         a = np.ascontiguousarray(data, dtype=np.complex128).reshape(self.shape).copy()
@@ -377,6 +426,17 @@ class Field:
     def set_cosmology(self, cosmo: int, ai: float = 1.0):
         """0: STATIC; 1: MRE from a = ai (the reference's --cosmo mre)."""
         self._c("qx_set_cosmology", cosmo, ai)
+
+    def cosmology(self):
+        """(mode, a, ds): 0 STATIC / 1 MRE, scale factor, current time step."""
+        c, a, ds = C.c_int(), C.c_double(), C.c_double()
+        self._c("qx_get_cosmology", C.byref(c), C.byref(a), C.byref(ds))
+        return c.value, a.value, ds.value
+
+    def restore_cosmology(self, a: float, ds: float):
+        """Restore the scale factor and time step of a checkpoint (after
+        set_cosmology, which starts the cosmology afresh)."""
+        self._c("qx_restore_cosmology", a, ds)
 
     def set_clock(self, step: int, time: float):
         """Set the step counter and time (restoring a checkpoint)."""
@@ -466,8 +526,18 @@ class Ensemble:
 
     def ic_config(self, kind: int = IC_GRF, seed_base: int = 1234, n_sol: int = 0, rc_lo: float = 0.01,
                   rc_hi: float = 0.03, sigma: float = 0.3, kc_factor: float = 0.125, clip: float = -0.9,
-                  rho0: float = 1e-6):
-        self._c("qx_ens_ic_config", kind, seed_base, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0)
+                  rho0: float = 1e-6, seeds=None):
+        """Initial conditions of every box: box b seeded with seed_base + b, or
+        with seeds[b] when a per-box seed list is given (a sharded ensemble
+        passes seed_base + its boxes' global indices)."""
+        if seeds is None:
+            self._c("qx_ens_ic_config", kind, seed_base, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0)
+            return
+        seeds = [int(x) for x in seeds]
+        if len(seeds) != self.nboxes:
+            raise ValueError(f"seeds holds {len(seeds)} values for {self.nboxes} boxes")
+        arr = (C.c_ulonglong * len(seeds))(*seeds)
+        self._c("qx_ens_ic_config_seeds", kind, arr, n_sol, rc_lo, rc_hi, sigma, kc_factor, clip, rho0)
 
     def psi(self, box: int) -> np.ndarray:
         a = np.empty(self.box_shape(box), np.complex128)
@@ -497,14 +567,23 @@ def shard_groups(groups, world: int, rank: int):
     the boxes, numbered group by group, are dealt out round-robin, so every
     rank gets a near-equal share of every size.  Returns (groups_of_rank,
     global box indices of rank) with groups_of_rank in the (N, count) form of
-    Ensemble (sizes with no box on this rank are left out)."""
-    boxes = []
+    Ensemble (groups with no box on this rank are left out) and the global
+    indices in the rank's local box order (Ensemble numbers its boxes group
+    by group): local box i of the rank's Ensemble is global box mine[i]."""
+    out, mine = [], []
+    start = 0
     for n, c in groups:
-        boxes += [int(n)] * int(c)
-    mine = [b for b in range(len(boxes)) if b % world == rank]
-    out = []
-    for n, _ in groups:
-        k = sum(1 for b in mine if boxes[b] == int(n))
-        if k:
-            out.append((int(n), k))
+        local = [b for b in range(start, start + int(c)) if b % world == rank]
+        if local:
+            out.append((int(n), len(local)))
+            mine += local
+        start += int(c)
     return out, mine
+
+
+def shard_seeds(groups, world: int, rank: int, seed_base: int):
+    """Per-box seeds of rank `rank`'s Ensemble (in its local box order): box b
+    of the whole ensemble is seeded with seed_base + b on whichever rank runs
+    it, so a sharded run simulates exactly the boxes of the unsharded one."""
+    _, mine = shard_groups(groups, world, rank)
+    return [seed_base + b for b in mine]

@@ -4,7 +4,8 @@ The reference's IO::writeConf / readConf (src/io/io.cxx:276-369) store, in
 HDF5, a Header group (N, dim, step, time, a, Lbox) and psi as real and
 imaginary double datasets in reference site order.  HDF5 is not used here: a
 checkpoint is `<path>.json` (the same header fields plus what a restart needs
-to rebuild the field: dtype, pref, rho_mean, dt, k0) and `<path>.psi`
+to rebuild the field: dtype, pref, rho_mean, dt, k0, the cosmology mode and
+the current time step ds) and `<path>.psi`
 (interleaved complex128, little-endian, reference site order, x fastest).
 """
 from __future__ import annotations
@@ -22,9 +23,10 @@ def save(field: Field, path: str, pref: float = 1.0, rho_mean: float = 1.0, k0: 
     """Write `path`.json and `path`.psi.  The physical constants of the field
     (pref, rho_mean, k0) are not readable back from a Field, so the caller
     states them."""
+    cosmo, a, ds = field.cosmology()
     hdr = {"format": FORMAT, "N": field.N_, "dim": field.dim_, "step": field.curr(), "time": field.time(),
-           "a": field.a(), "Lbox": field.L, "dtype": field.dtype, "pref": pref, "rho_mean": rho_mean,
-           "dt": field.dt(), "k0": k0}
+           "a": a, "Lbox": field.L, "dtype": field.dtype, "pref": pref, "rho_mean": rho_mean,
+           "dt": field.dt(), "k0": k0, "cosmo": cosmo, "ds": ds}
     psi = field.psi
     psi.astype("<c16").tofile(path + ".psi")
     with open(path + ".json", "w") as fh:
@@ -45,5 +47,10 @@ def load(path: str, dtype: str | None = None) -> Field:
         f.close()
         raise ValueError(f"{path}.psi holds {psi.size} values, expected {N**dim}")
     f.psi = psi.reshape((N,) * dim)
+    if int(hdr.get("cosmo", 0)) == 1:
+        # MRE: set_cosmology sets rho_mean and the Poisson prefactor's mode and
+        # starts a afresh; then the checkpoint's a and ds are put back
+        f.set_cosmology(1, float(hdr["a"]))
+        f.restore_cosmology(float(hdr["a"]), float(hdr["ds"]))
     f.set_clock(int(hdr["step"]), float(hdr["time"]))
     return f

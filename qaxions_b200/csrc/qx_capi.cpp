@@ -329,6 +329,73 @@ int qx_set_cosmology(qx_field_t* h, int cosmo, double ai) {
     return guarded(h, [&](qx::Field& f) { f.set_cosmology(cosmo, ai); });
 }
 
+static void to_c(const qx::MeasRecord& r, qx_meas_t* o) {
+    o->number = r.number;
+    o->step = r.step;
+    o->time = r.time;
+    o->a = r.a;
+    o->rhomax = r.rhomax;
+    o->vmax = r.vmax;
+    o->mass = r.mass;
+    o->energy = r.energy;
+    o->kinetic = r.kinetic;
+    o->potential = r.potential;
+}
+
+int qx_meas_list(long long nsteps, long long nmeas, long long* out, int max_out, int* n_out) {
+    if (nsteps < 0 || nmeas < 0 || max_out < 0 || (max_out > 0 && !out)) {
+        g_err = "nsteps, nmeas and max_out must be >= 0 and out not NULL";
+        return QX_ERR_INVALID;
+    }
+    const auto ml = qx::meas_list((long)nsteps, (long)nmeas);
+    if ((long long)ml.size() > max_out) {
+        g_err = "out holds fewer than nmeas entries";
+        return QX_ERR_INVALID;
+    }
+    for (size_t i = 0; i < ml.size(); ++i) out[i] = ml[i];
+    if (n_out) *n_out = (int)ml.size();
+    g_err.clear();
+    return QX_OK;
+}
+
+int qx_measure(qx_field_t* h, unsigned mask, int number, const char* dir, qx_meas_t* rec) {
+    return guarded(h, [&](qx::Field& f) {
+        need(number >= 0, "number must be >= 0");
+        qx::MeasRecord r;
+        f.measure(mask, number, dir, &r);
+        if (rec) to_c(r, rec);
+    });
+}
+
+int qx_run(qx_field_t* h, int nsteps, int nmeas, unsigned mask, const char* dir, qx_meas_t* recs, int max_recs,
+           int* n_out) {
+    return guarded(h, [&](qx::Field& f) {
+        need(nsteps >= 0 && nmeas >= 0, "nsteps and nmeas must be >= 0");
+        need(max_recs >= 0 && (max_recs == 0 || recs), "recs must hold max_recs records");
+        need(mask == QX_MEAS_NONE || max_recs >= nmeas + 1, "recs must hold nmeas + 1 records");
+        std::vector<qx::MeasRecord> out;
+        f.run(nsteps, nmeas, mask, dir, out);
+        for (size_t i = 0; i < out.size() && (int)i < max_recs; ++i) to_c(out[i], &recs[i]);
+        if (n_out) *n_out = (int)out.size();
+    });
+}
+
+int qx_get_cosmology(qx_field_t* h, int* cosmo, double* a, double* ds) {
+    return guarded(h, [&](qx::Field& f) {
+        if (cosmo) *cosmo = f.cosmology();
+        if (a) *a = f.a();
+        if (ds) *ds = f.dt();
+    });
+}
+
+int qx_restore_cosmology(qx_field_t* h, double a, double ds) {
+    return guarded(h, [&](qx::Field& f) {
+        need(std::isfinite(a) && a > 0 && std::isfinite(ds), "a must be finite and > 0, ds finite");
+        need(f.cosmology() == 1 || a == 1.0, "a STATIC field keeps a = 1");
+        f.restore_cosmology(a, ds);
+    });
+}
+
 int qx_set_clock(qx_field_t* h, int step, double time) {
     return guarded(h, [&](qx::Field& f) {
         need(step >= 0 && std::isfinite(time), "step must be >= 0 and time finite");
@@ -482,6 +549,18 @@ int qx_ens_ic_config(qx_ens_t* h, int kind, unsigned long long seed_base, int n_
         need(n_sol >= 0, "n_sol must be >= 0");
         for (size_t i = 0; i < e.group_of.size(); ++i)
             e.groups[e.group_of[i]]->ic_config_box(e.index_in[i], kind, seed_base + i, n_sol, rc_lo, rc_hi, sigma,
+                                                   kc_factor, clip, rho0);
+    });
+}
+
+int qx_ens_ic_config_seeds(qx_ens_t* h, int kind, const unsigned long long* seeds, int n_sol, double rc_lo,
+                           double rc_hi, double sigma, double kc_factor, double clip, double rho0) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(kind == QX_IC_GRF || kind == QX_IC_SOLITONS, "kind must be QX_IC_GRF or QX_IC_SOLITONS");
+        need(n_sol >= 0, "n_sol must be >= 0");
+        need(seeds != nullptr, "seeds must not be NULL");
+        for (size_t i = 0; i < e.group_of.size(); ++i)
+            e.groups[e.group_of[i]]->ic_config_box(e.index_in[i], kind, seeds[i], n_sol, rc_lo, rc_hi, sigma,
                                                    kc_factor, clip, rho0);
     });
 }

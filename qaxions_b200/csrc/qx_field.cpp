@@ -2,8 +2,10 @@
 #include "qx_field.hpp"
 
 #include <cmath>
+#include <limits>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <map>
 #include <sstream>
 #include <stdexcept>
@@ -454,10 +456,22 @@ class FieldT final : public Field {
     void y_inv(C* a, int X) {
         if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp(a, X), +1, tune_, st_);
     }
+    // drift factor tables A(nx, ny), B(nz)/S for time step dt (recomputed only
+    // when dt changes; capture_body computes them before a capture begins)
+    const double2* ensure_axy(double dt) {
+        const double fac = -0.5 * dt * dk() * dk();
+        if (!axy_.p) axy_.alloc(sizeof(double2) * (size_t)g_.N * ((g_.dim == 3 ? g_.N : 1) + 1));
+        if (!(axy_fac_ == fac)) {
+            drift_tables(axy_.as<double2>(), g_.dim, g_.N, fac, 1.0 / (double)g_.S1, st_);
+            axy_fac_ = fac;
+        }
+        return axy_.as<double2>();
+    }
     void la_drift(double dt) {
         auto s = sp(psi(), g_.N);
         s.phase_fac = -0.5 * dt * dk() * dk();
         s.scale = 1.0 / (double)g_.S1;
+        s.axy = ensure_axy(dt);
         Ops<R>::la_pass(g_.N, s, OP_DRIFT, tune_, st_);
     }
     // psi^_x -> y forward, z drift, y inverse: one slab-ordered kernel (FP32
@@ -530,22 +544,25 @@ class FieldT final : public Field {
         v_current_ = false;
     }
 
-    // fused merged leapfrog (src/main.cxx:64-85)
-    void step(int nsteps) override {
-        if (nsteps <= 0) return;
-        // prologue: potential of psi, half kick, forward x transform
+    // prologue of the merged loop: potential of psi, half kick, forward x
+    // transform (psi left transformed along x for the first drift)
+    void prologue() {
         density_r2c_partial();
         la_poisson();
         y_inv(vh(), g_.N / 2);
-        {
-            auto a = xp();
-            a.in = psi();
-            a.out = psi();
-            a.vh = vh();
-            a.Vout = V();
-            a.dt = 0.5 * ds_;
-            Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_);
-        }
+        auto a = xp();
+        a.in = psi();
+        a.out = psi();
+        a.vh = vh();
+        a.Vout = V();
+        a.dt = 0.5 * ds_;
+        Ops<R>::x_c2r(g_.N, a, C2R_KICK | C2R_FWD, tune_, st_);
+    }
+
+    // fused merged leapfrog (src/main.cxx:64-85)
+    void step(int nsteps) override {
+        if (nsteps <= 0) return;
+        prologue();
         if (cosmo_ == 1) {
             // MRE: every step has its own drift step, prefactor (norm a) and
             // kick step (after updateTime), so the body runs without the graph
@@ -565,8 +582,7 @@ class FieldT final : public Field {
                 }
             }
             body(ds_, ds_, pref_eff(), true);
-            curr_ += nsteps;
-            s_ += nsteps * ds_;
+            for (int i = 0; i < nsteps; ++i) updateTime();  // curr_ and s_ as the reference advances them
         }
         v_current_ = true;
         vmax_stale_ = true;
@@ -599,8 +615,160 @@ class FieldT final : public Field {
         }
     }
 
+    // ---- measured time loop (src/main.cxx:60-85, src/meas.cxx:13-63) ----
+
+    // loop body up to the potential: drift, density, Poisson, c2r -> V; psi
+    // stays in real space (the state measure() sees after drift_update)
+    void body_to_potential(double dt, double pref) {
+        yz_drift(dt);
+        auto a = xp();
+        a.in = psi();
+        a.out = psi();
+        a.vh = vh();
+        a.Vout = V();
+        a.pref = pref;
+        a.rho_mean = cfg_.rho_mean;
+        Ops<R>::x_inv(g_.N, a, true, tune_, st_);
+        y_fwd(vh(), g_.N / 2);
+        la_poisson();
+        y_inv(vh(), g_.N / 2);
+        Ops<R>::x_c2r(g_.N, a, C2R_WRITE_V, tune_, st_);
+    }
+
+    void measure(unsigned mask, int number, const char* dir, MeasRecord* rec) override {
+        MeasRecord r;
+        r.number = number;
+        r.step = curr_;
+        r.time = s_;
+        r.a = a_;
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        r.mass = r.energy = r.kinetic = r.potential = nan;
+        if (mask == MEAS_NONE) {  // src/meas.cxx:18-19
+            if (rec) *rec = r;
+            return;
+        }
+        single_box("measure");
+        // computeEnergy's rhomax (src/meas.cxx:30), without overwriting V
+        auto rr = reduce(RED_RHO);
+        rhomax_ = rr[1] / (rr[0] / (double)g_.S);
+        r.rhomax = rhomax_;
+        ensure_V();
+        vmax_ = reduce(RED_VABS)[1];
+        vmax_stale_ = false;
+        r.vmax = vmax_;
+        if (mask & MEAS_ENERGY) mass_energy(&r.mass, &r.energy, &r.kinetic, &r.potential);
+        const std::string d = dir ? dir : "";
+        auto fname = [&](const char* stem, const char* ext) {
+            std::ostringstream o;
+            o << d << "/" << stem << "_" << std::setw(4) << std::setfill('0') << number << ext;
+            return o.str();
+        };
+        if ((mask & MEAS_SPECTRUM) && dir) {
+            // Spectrum of rho = |psi|^2 (the V_ that computeEnergy leaves), written
+            // like Spectrum::write (src/spectrum/spectrum.cxx:167-183)
+            const int nb = g_.N / 2 + 1;
+            std::vector<double> k(nb), P(nb);
+            std::vector<long long> c(nb);
+            spectrum(0, 0, nb, k.data(), P.data(), c.data());
+            std::ofstream out(fname("spec", ".txt"));
+            if (!out) throw std::invalid_argument("cannot open " + fname("spec", ".txt"));
+            out << "# a: " << a_ << "\n";
+            out << "# k_phys      P(k)          count\n";
+            out << std::scientific;
+            for (int b = 0; b < nb; ++b)
+                if (c[b] != 0) out << k[b] << "  " << P[b] << "  " << c[b] << "\n";
+        }
+        if ((mask & MEAS_RHO_GRID) && dir) {
+            // the density grid of IO::writeConf (src/io/io.cxx:314-340) as raw
+            // FP64 in reference order, with its Header fields in a JSON file
+            std::vector<double> rho(g_.S);
+            std::vector<double> hp(2 * (size_t)g_.S);
+            get_psi(hp.data());
+            for (long i = 0; i < g_.S; ++i) rho[i] = hp[2 * i] * hp[2 * i] + hp[2 * i + 1] * hp[2 * i + 1];
+            std::ofstream out(fname("field", ".rho"), std::ios::binary);
+            if (!out) throw std::invalid_argument("cannot open " + fname("field", ".rho"));
+            out.write(reinterpret_cast<const char*>(rho.data()), sizeof(double) * rho.size());
+            std::ofstream hdr(fname("field", ".json"));
+            hdr << std::setprecision(17) << "{\"N\": " << g_.N << ", \"dim\": " << g_.dim << ", \"step\": " << curr_
+                << ", \"time\": " << s_ << ", \"a\": " << a_ << ", \"Lbox\": " << cfg_.L << "}\n";
+        }
+        if (dir) {
+            std::ofstream js(d + "/measurements.jsonl", number == 0 ? std::ios::trunc : std::ios::app);
+            if (!js) throw std::invalid_argument("cannot open " + d + "/measurements.jsonl");
+            js << std::setprecision(17) << "{\"number\": " << r.number << ", \"step\": " << r.step
+               << ", \"time\": " << r.time << ", \"a\": " << r.a << ", \"rhomax\": " << r.rhomax
+               << ", \"vmax\": " << r.vmax;
+            if (mask & MEAS_ENERGY)
+                js << ", \"mass\": " << r.mass << ", \"energy\": " << r.energy << ", \"kinetic\": " << r.kinetic
+                   << ", \"potential\": " << r.potential;
+            js << "}\n";
+        }
+        if (mask & MEAS_CLOBBER_V) computeEnergy();  // V <- |psi|^2 as the reference's measure leaves it
+        if (rec) *rec = r;
+    }
+
+    void run(int nsteps, int nmeas, unsigned mask, const char* dir, std::vector<MeasRecord>& out) override {
+        if (nsteps < 0 || nmeas < 0) throw std::invalid_argument("nsteps and nmeas must be >= 0");
+        const auto ml = meas_list(nsteps, nmeas);
+        out.clear();
+        MeasRecord r;
+        measure(mask, 0, dir, &r);  // src/main.cxx:64
+        if (mask != MEAS_NONE) out.push_back(r);
+        if (nsteps == 0) return;
+        v_current_ = false;  // src/main.cxx:65: the loop starts from updatePotential
+        prologue();          // updatePotential, half_kick (src/main.cxx:65-69), x forward
+        size_t next = 0;
+        int number = 0;
+        for (int idx = 0; idx < nsteps; ++idx) {
+            const bool last = idx == nsteps - 1;
+            const bool meas = next < ml.size() && (long)idx == ml[next];
+            const double dt_drift = ds_;
+            if (!meas) {
+                if (cosmo_ == 1) {
+                    updateTime();
+                    body(dt_drift, ds_, pref_eff(), last);
+                } else {
+                    if (!last && graph_enabled_) {
+                        if (!graph_exec_ || graph_dt_ != ds_) capture_body();
+                        QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
+                    } else {
+                        body(ds_, ds_, pref_eff(), last);
+                    }
+                    updateTime();
+                }
+                continue;
+            }
+            // drift_update (drift, updateTime, updatePotential), then measure
+            if (cosmo_ == 1) updateTime();
+            body_to_potential(dt_drift, pref_eff());
+            if (cosmo_ != 1) updateTime();
+            v_current_ = true;
+            vmax_stale_ = true;
+            ++next;
+            measure(mask, ++number, dir, &r);  // src/main.cxx:75-79
+            out.push_back(r);
+            auto a = xp();
+            a.in = psi();
+            a.out = psi();
+            a.Vin = V();
+            if (!last) {  // full_kick, then x forward for the next drift
+                a.dt = ds_;
+                Ops<R>::x_fwd(g_.N, a, true, tune_, st_);
+            } else {      // the final half_kick (src/main.cxx:82)
+                Misc<R>::kick(psi(), V(), 0.5 * ds_, g_.S, st_);
+            }
+        }
+        // V is the potential of psi unless the last step was measured with
+        // MEAS_CLOBBER_V (then it holds rho, as the reference leaves it)
+        const bool last_measured = next > 0 && ml[next - 1] == (long)nsteps - 1;
+        v_current_ = !(last_measured && (mask & MEAS_CLOBBER_V));
+        vmax_stale_ = true;
+        QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
     void capture_body() {
         drop_graph();
+        ensure_axy(ds_);  // the drift table is an input of the graph, not part of it
         // one eager launch first so kernel attributes are set outside capture
         QX_CUDA(cudaStreamSynchronize(st_));
         cudaGraph_t g;
@@ -1190,6 +1358,8 @@ class FieldT final : public Field {
     DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, twNn_, red_, redout_, errbuf_;
     TwTables<C> tw_{};
     int* err_ = nullptr;
+    DevBuf axy_;       // drift factor tables A(nx, ny), B(nz)/S (ensure_axy)
+    double axy_fac_ = std::numeric_limits<double>::quiet_NaN();
     DevBuf chain_;     // drift chain: [3n] phase counters
     int chain_n_ = 0;  // 8-column slabs of the drift chain (0: three separate passes)
     DevBuf mpsi_, mvh_, kin_, specP_, specC_, stage_;
@@ -1201,6 +1371,15 @@ class FieldT final : public Field {
     cudaGraphExec_t graph_exec_ = nullptr;
     double graph_dt_ = 0.0;
 };
+
+std::vector<long> meas_list(long nsteps, long nmeas) {  // src/utils.cxx:8-28
+    std::vector<long> out;
+    if (nmeas <= 0 || nsteps <= 0) return out;
+    if (nmeas == 1) return {nsteps - 1};
+    out.reserve(nmeas);
+    for (long k = 0; k < nmeas; ++k) out.push_back(k * (nsteps - 1) / (nmeas - 1));
+    return out;
+}
 
 std::unique_ptr<Field> make_field(const FieldConfig& cfg) {
     if (cfg.prec == Prec::F64) return std::make_unique<FieldT<double>>(cfg);

@@ -105,6 +105,33 @@ class B200FFTBackend : public FFTBackend {
     int* err_;  // device flag raised by a timed-out wait in a pass kernel
 };
 
+// MeasureType bits (src/enum.h:39-47) plus this library's own
+enum MeasBits : unsigned {
+    MEAS_NONE = 0,
+    MEAS_SPECTRUM = 1u << 0,   // spec_NNNN.txt of |psi|^2, reference shells
+    MEAS_RHO_MAX = 1u << 1,    // (rhomax is measured whenever the mask is not NONE)
+    MEAS_RHO_SLICE = 1u << 2,  // enumerated by the reference, not acted on by its measure()
+    MEAS_RHO_GRID = 1u << 3,   // field_NNNN.rho (raw FP64 density) + field_NNNN.json header
+    MEAS_PSI_GRID = 1u << 4,   // enumerated by the reference, not acted on by its measure()
+    MEAS_ENERGY = 1u << 8,     // mass, kinetic and potential energy (no reference counterpart)
+    MEAS_CLOBBER_V = 1u << 9,  // reproduce the reference's V <- |psi|^2 before the next kick
+};
+
+// one measurement (the quantities measure()/printStatus report, plus ours)
+struct MeasRecord {
+    int number = 0;      // measurement number (0: before the time loop)
+    int step = 0;        // Field::curr()
+    double time = 0.0;   // Field::time()
+    double a = 1.0;      // Field::a()
+    double rhomax = 0.0; // computeEnergy: max |psi|^2 / mean |psi|^2
+    double vmax = 0.0;   // max |V| of the potential of this psi
+    double mass = 0.0, energy = 0.0, kinetic = 0.0, potential = 0.0;  // MEAS_ENERGY, else NaN
+};
+
+// generateMeasList (src/utils.cxx:8-28): the loop indices after whose
+// drift_update a measurement is taken
+std::vector<long> meas_list(long nsteps, long nmeas);
+
 class Field {
   public:
     virtual ~Field() = default;
@@ -126,6 +153,13 @@ class Field {
     // merged leapfrog of src/main.cxx:64-85 (measurements off), fused passes,
     // loop body replayed from a CUDA graph
     virtual void step(int nsteps) = 0;
+    // measure() (src/meas.cxx:13-63) without overwriting V (unless the mask
+    // has MEAS_CLOBBER_V); files go to `dir` when it is not null
+    virtual void measure(unsigned mask, int number, const char* dir, MeasRecord* rec) = 0;
+    // the time loop of main() (src/main.cxx:64-85) with its measurements:
+    // measure(0), then one measurement after the drift_update of every loop
+    // index of meas_list(nsteps, nmeas); records in `out`
+    virtual void run(int nsteps, int nmeas, unsigned mask, const char* dir, std::vector<MeasRecord>& out) = 0;
 
     // ---- buffers (host FP64, reference index order) ----
     virtual void set_psi(const double* interleaved) = 0;
@@ -193,6 +227,13 @@ class Field {
     double a() const { return a_; }
     double dt() const { return ds_; }
     void set_dt(double dt) { ds_ = dt; }
+    // restore the scale factor and time step of a checkpoint (after
+    // set_cosmology, which resets them to the start of the cosmology)
+    void restore_cosmology(double a, double ds) {
+        a_ = a;
+        ds_ = ds;
+        invalidate_graph();
+    }
     // restore the step counter and time of a checkpoint
     void set_clock(int step, double time) {
         curr_ = step;

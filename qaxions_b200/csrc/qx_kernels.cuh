@@ -116,17 +116,17 @@ template <typename C> __device__ __forceinline__ C cmul_d(C v, double2 w) {
     return mk<C>((decltype(C::x))fma(vx, w.x, -vy * w.y), (decltype(C::x))fma(vx, w.y, vy * w.x));
 }
 
-// psi * exp(-i dt V)   (src/field.cxx:100-112).  FP64: phase reduced mod 2 pi
-// in FP64.  FP32: the phase -dt V is formed in FP32 (one rounding, the size of
-// V's own FP32 representation error) and reduced by sincosf itself.
+// psi * exp(-i dt V)   (src/field.cxx:100-112).  Both forms form the phase
+// -dt V in FP64 and reduce it mod 2 pi there; the FP32 form then rounds the
+// reduced phase (|phi| <= pi) once and takes sincosf of it.  Forming dt V in
+// FP32 instead would round dt itself (a fixed relative error applied at
+// every step) and lose |dt V| 6e-8 of absolute phase to the product.
 template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, double dt);
 template <> __device__ __forceinline__ double2 kick1<double>(double2 p, double v, double dt) {
     return cmul(p, cis<double>(-dt * v));
 }
 template <> __device__ __forceinline__ float2 kick1<float>(float2 p, float v, double dt) {
-    float s, c;
-    sincosf((float)(-dt) * v, &s, &c);
-    return cmul(p, make_float2(c, s));
+    return cmul(p, cis<float>(-dt * (double)v));
 }
 
 __device__ __forceinline__ int signed_mode(int i, int N) { return i <= (N >> 1) ? i : i - N; }
@@ -156,8 +156,12 @@ template <typename C> __device__ __forceinline__ void store_pair(C* row, int q, 
 // deterministic block reductions (fixed tree, FP64)
 // ---------------------------------------------------------------------------
 
-template <int OP>  // 0 sum, 1 max
-__device__ __forceinline__ double red_op(double a, double b) { return OP == 0 ? a + b : fmax(a, b); }
+// max that keeps a NaN from either side: a NaN density or potential must show
+// up in the diagnostics instead of being hidden behind a finite maximum
+__device__ __forceinline__ double fmax_nan(double a, double b) { return (a > b || a != a) ? a : b; }
+
+template <int OP>  // 0 sum, 1 max (NaN-propagating)
+__device__ __forceinline__ double red_op(double a, double b) { return OP == 0 ? a + b : fmax_nan(a, b); }
 
 template <int OP>
 __device__ double block_reduce(double v, double* red) {
@@ -181,6 +185,18 @@ __device__ double block_reduce(double v, double* red) {
     for (int w = 1; w < nthr; ++w) r = red_op<OP>(r, red[w]);
     __syncthreads();
     return r;
+}
+
+// One warp folds n per-block partials in a fixed order (deterministic): lane l
+// takes l, l + 32, ... in turn, then a fixed shuffle tree; every lane returns
+// the result.  Call with all 32 lanes of the warp.
+template <int OP>
+__device__ __forceinline__ double warp_fold(const double* p, long n) {
+    double v = OP == 0 ? 0.0 : -CUDART_INF;
+    for (long i = threadIdx.x & 31; i < n; i += 32) v = red_op<OP>(v, p[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = red_op<OP>(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
 // ---------------------------------------------------------------------------

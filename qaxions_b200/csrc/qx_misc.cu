@@ -86,9 +86,9 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce(int kind, const cx_t<R>*
             const cx_t<R> p = psi[i];
             const double r = (double)p.x * p.x + (double)p.y * p.y;
             a0 += r;
-            a1 = fmax(a1, r);
+            a1 = fmax_nan(a1, r);
         } else if (kind == RED_VABS) {
-            a1 = fmax(a1, fabs((double)V[i]));
+            a1 = fmax_nan(a1, fabs((double)V[i]));
         } else if (kind == RED_VRHO) {
             const cx_t<R> p = psi[i];
             a0 += (double)V[i] * ((double)p.x * p.x + (double)p.y * p.y);
@@ -107,24 +107,41 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce(int kind, const cx_t<R>*
     }
 }
 
+// one warp (launched <<<1, 32>>>) folds the per-block partials
 __global__ void k_fold(const double* partial, int n, double* out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0, m = 0.0;
-        for (int i = 0; i < n; ++i) {
-            s += partial[i];
-            m = fmax(m, partial[n + i]);
-        }
+    const double s = warp_fold<0>(partial, n);
+    const double m = warp_fold<1>(partial + n, n);
+    if (threadIdx.x == 0) {
         out[0] = s;
         out[1] = m;
     }
 }
 
 __global__ void k_fold_sum(const double* partial, long n, double* out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (long i = 0; i < n; ++i) s += partial[i];
-        out[0] = s;
+    const double s = warp_fold<0>(partial, n);
+    if (threadIdx.x == 0) out[0] = s;
+}
+
+// drift factor tables (qx_misc.hpp)
+__global__ void k_drift_tables(double2* t, int dim, int N, double fac, double scale) {
+    const long na = dim == 3 ? (long)N * N : N;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < na + N; i += (long)gridDim.x * blockDim.x) {
+        if (i < na) {
+            const long nx = signed_mode((int)(i % N), N);
+            const long ny = dim == 3 ? signed_mode((int)(i / N), N) : 0;
+            t[i] = cis_d(fac * (double)(nx * nx + ny * ny));
+        } else {
+            const long n = signed_mode((int)(i - na), N);
+            const double2 w = cis_d(fac * (double)(n * n));
+            t[i] = make_double2(w.x * scale, w.y * scale);
+        }
     }
+}
+
+void drift_tables(double2* t, int dim, int N, double fac, double scale, cudaStream_t st) {
+    const long n = (dim == 3 ? (long)N * N : N) + N;
+    k_drift_tables<<<grid_for(n, 256), 256, 0, st>>>(t, dim, N, fac, scale);
+    QX_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------

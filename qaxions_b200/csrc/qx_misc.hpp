@@ -49,6 +49,12 @@ template <typename R> struct Misc {
     static void scale(C* psi, double s, long n, cudaStream_t st);
 };
 
+// drift factor tables of exp(i fac |n|^2) / S = A(nx, ny) B(nz) (FP64,
+// arguments reduced mod 2 pi): A = exp(i fac (nx^2 + ny^2)) at t[y * N + x]
+// for x < N and y < N (3D) or y = 0 (2D), then B = exp(i fac n^2) * scale at
+// t[rowsA * N + i] for i < N (rowsA = N in 3D, 1 in 2D)
+void drift_tables(double2* t, int dim, int N, double fac, double scale, cudaStream_t st);
+
 // initial-condition kernels (FP64 only)
 struct IC {
     // psi = (g, 0), g standard normal from Philox (counter (i, 0, stream, 0))

@@ -12,11 +12,15 @@
 // held by every GPU that loads this library until the process exits).  Host
 // code must not pass the array's name to a kernel: on the host that name is
 // only a stand-in, not a device address.  The device address is looked up
-// once per device with cudaGetSymbolAddress while that device is current (on
-// the first call made for that device; make that first call before any stream
-// capture begins).  Every call writes each partial slot it later reads, so
-// nothing needs clearing between calls; calls that overlap on the GPU share
-// the array and race.
+// with cudaGetSymbolAddress while the device is current, on the first call
+// made for that device (make that first call before any stream capture
+// begins), and looked up again only if the device's context has changed
+// since (a cudaDeviceReset between calls gives the device a new context in
+// which the array has a new address).  Every call writes each partial slot it
+// later reads, so nothing needs clearing between calls; calls that overlap on
+// the GPU share the array and race.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -35,7 +39,11 @@ constexpr int kMaxDevices = 64;
 // two partials (sum, max) per block
 static __device__ __align__(256) double g_noalloc_partials[2 * kMaxBlocks];
 
-double* g_partials_addr[kMaxDevices] = {};
+struct DevScratch {
+    double* addr = nullptr;
+    unsigned long long ctx_id = 0;  // context in which addr was looked up
+};
+DevScratch g_scratch[kMaxDevices];
 std::mutex g_mu;
 thread_local std::string g_err;
 
@@ -51,7 +59,7 @@ __global__ void __launch_bounds__(kThreads) k_rho_partials(const qx::cx_t<R>* ps
             const qx::cx_t<R> p = psi[i];
             const double r = (double)p.x * p.x + (double)p.y * p.y;
             s += r;
-            m = fmax(m, r);
+            m = qx::fmax_nan(m, r);
         }
     }
     const double bs = qx::block_reduce<0>(s, red);
@@ -62,17 +70,57 @@ __global__ void __launch_bounds__(kThreads) k_rho_partials(const qx::cx_t<R>* ps
     }
 }
 
+// one warp folds the block partials in a fixed order (NaN-propagating max)
 __global__ void k_rho_fold(const double* part, int nblk, long n, double* out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0, m = 0.0;
-        for (int b = 0; b < nblk; ++b) {
-            s += part[b];
-            m = fmax(m, part[kMaxBlocks + b]);
-        }
+    const double s = qx::warp_fold<0>(part, nblk);
+    const double m = qx::warp_fold<1>(part + kMaxBlocks, nblk);
+    if (threadIdx.x == 0) {
         out[0] = s;
         out[1] = m;
         out[2] = m / (s / (double)n);
     }
+}
+
+template <typename F> F driver_fn(const char* name) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return reinterpret_cast<F>(p);
+}
+
+// `ptr` .. `ptr + bytes` must lie inside one device allocation of device `dev`
+bool device_extent_ok(const void* ptr, size_t bytes, int dev, const char* what) {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, ptr) != cudaSuccess ||
+        (pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != dev) {
+        cudaGetLastError();
+        g_err = std::string(what) + " is not device memory of the current device (select it with qx_set_device)";
+        return false;
+    }
+    static const auto range = driver_fn<PFN_cuMemGetAddressRange_v3020>("cuMemGetAddressRange");
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (!range || range(&base, &size, reinterpret_cast<CUdeviceptr>(ptr)) != CUDA_SUCCESS) {
+        g_err = std::string("cannot determine the allocation that holds ") + what;
+        return false;
+    }
+    const uintptr_t p = reinterpret_cast<uintptr_t>(ptr);
+    if (p < (uintptr_t)base || p - (uintptr_t)base > size || bytes > size - (p - (uintptr_t)base)) {
+        g_err = std::string(what) + " extends past the end of its device allocation";
+        return false;
+    }
+    return true;
+}
+
+// id of the current context (0 if it cannot be read)
+unsigned long long current_ctx_id() {
+    static const auto get_cur = driver_fn<PFN_cuCtxGetCurrent_v4000>("cuCtxGetCurrent");
+    static const auto get_id = driver_fn<PFN_cuCtxGetId_v12000>("cuCtxGetId");
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur && get_id && get_cur(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS) return id;
+    return 0;
 }
 
 }  // namespace
@@ -98,25 +146,26 @@ extern "C" int qx_rho_stats_noalloc(const void* psi, long long sites, int dtype,
         g_err = "no usable current CUDA device";
         return QX_ERR_CUDA;
     }
-    cudaPointerAttributes pa;
-    if (cudaPointerGetAttributes(&pa, psi) != cudaSuccess || pa.type != cudaMemoryTypeDevice || pa.device != dev) {
-        cudaGetLastError();
-        g_err = "psi is not device memory of the current device (select it with qx_set_device)";
-        return QX_ERR_INVALID;
-    }
+    const size_t elem = dtype == QX_C64 ? sizeof(float2) : sizeof(double2);
+    if (!device_extent_ok(psi, (size_t)sites * elem, dev, "psi")) return QX_ERR_INVALID;
+    if (!device_extent_ok(out, 3 * sizeof(double), dev, "out")) return QX_ERR_INVALID;
     double* part = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_partials_addr[dev]) {
+        const unsigned long long ctx = current_ctx_id();
+        DevScratch& ds = g_scratch[dev];
+        if (!ds.addr || ds.ctx_id != ctx) {
             void* p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
             if (e != cudaSuccess || !p) {
+                cudaGetLastError();
                 g_err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
                 return QX_ERR_CUDA;
             }
-            g_partials_addr[dev] = static_cast<double*>(p);
+            ds.addr = static_cast<double*>(p);
+            ds.ctx_id = ctx;
         }
-        part = g_partials_addr[dev];
+        part = ds.addr;
     }
     const int nblk = (int)((sites + (long long)kThreads * kPerThread - 1) / ((long long)kThreads * kPerThread));
     cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -39,6 +39,9 @@ template <typename R> struct Ops {
         int batch;  // boxes stacked in the array (0 or 1: a single box)
         double phase_fac, scale, pois_c, pois_g0; double* partial;
         int* err;  // device flag set when a bounded wait times out
+        // drift: the factor tables A(nx, ny), B(nz) of drift_tables (qx_misc.hpp);
+        // the TMA drift pass reads them
+        const double2* axy;
     };
     static void x_fwd(int N, const XP& a, bool kick, const Tune& tu, cudaStream_t st);
     static void x_inv(int N, const XP& a, bool r2c, const Tune& tu, cudaStream_t st);

@@ -247,6 +247,7 @@ static TmaGeom tma_geom(int X, int want_tx, int op, const Tune& tu) {
     // a 3-deep ring, which lets two FP32 blocks share an SM (measured best at
     // 512^3 against 16 columns / deeper rings)
     int tx = want_tx > 0 ? want_tx : 8;
+    if (tx > kTmaMaxTX) tx = kTmaMaxTX;
     while (tx > PW && ((X % tx) || (tx / PW) * g.T > tma_max_threads<PW>())) tx >>= 1;
     if (TXF > 0) {  // compiled-in tile width
         tx = TXF;
@@ -304,6 +305,8 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.pois_c = a.pois_c;
     s.pois_g0 = a.pois_g0;
     s.col0_external = col0_ext;
+    s.axy = a.axy;
+    if (OP == OP_DRIFT && !a.axy) throw std::logic_error("drift pass needs the A(nx, ny) table");
     s.partial = a.partial;
     s.err = a.err;
     constexpr bool SWZ = tma_swizzled<NN, R, PW, TXF>();

@@ -14,6 +14,8 @@
 // in shared memory once per launch.  The drift phase exp(-i dt/2 dk^2 |n|^2)/S
 // is factored exactly as A(nx, ny) * B(nz); both factors are evaluated in FP64
 // with the argument reduced mod 2 pi, multiplied in FP64 and rounded once.
+// Both come from per-grid tables (drift_tables, computed once per time step
+// size); B is staged in shared memory once per launch.
 //
 // Every mbarrier wait is bounded (~1 s of SM clock); on time-out the kernel
 // sets *err, waits (bounded) for its own loads still in flight and for its
@@ -126,14 +128,18 @@ template <int N, typename R, int PW, int TXF> __host__ __device__ constexpr int 
 
 __host__ __device__ constexpr size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
 
+// widest tile (columns) of a strided pass: the drift pass keeps one A(nx, ny)
+// slot of this many double2 per ring buffer
+constexpr int kTmaMaxTX = 16;
+
 // dynamic shared memory of a pass: NBUF tiles + twiddles + drift factors
 // (drift only) + column-0 stash (Poisson only) + 128-byte base-alignment slack (the
 // tensor-copy alignment of unswizzled tiles; tiles are 1 KB multiples)
 template <typename R> __host__ __device__ constexpr size_t tma_smem_bytes(int N, int TX, int nbuf, int op,
                                                                           bool swz = false) {
     return (size_t)nbuf * align1k((size_t)N * TX * 2 * sizeof(R)) + (size_t)N * 4 * sizeof(R) +
-           (op == OP_DRIFT ? (size_t)N * 16 : 0) + (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) +
-           (swz ? 1024 : 128);
+           (op == OP_DRIFT ? (size_t)N * 16 + (size_t)nbuf * kTmaMaxTX * 16 : 0) +
+           (op == OP_POISSON ? (size_t)N * 2 * sizeof(R) : 0) + (swz ? 1024 : 128);
 }
 
 template <typename R> struct TArgs {
@@ -149,6 +155,7 @@ template <typename R> struct TArgs {
     long n_tiles;
     double phase_fac, scale, pois_c, pois_g0;
     int col0_external;   // 3D Poisson: column 0 is finished by k_poisson_col0
+    const double2* axy;  // drift: A(nx, ny) table [y][x] (x < N; y < N in 3D), then B(nz) / S
     double* partial;     // OP_KIN per-block sums
     int* err;            // set to 1 when a wait timed out
 };
@@ -209,7 +216,13 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
     C* tws = bufs + s.nbuf * tile_elems;
     C* tws_lo = tws + N;
     double2* bz = reinterpret_cast<double2*>(tws_lo + N);
-    C* col0 = reinterpret_cast<C*>(bz + (OP == OP_DRIFT ? N : 0));
+    double2* aslot = bz + N;  // drift: A(nx, ny) of each ring buffer's tile columns
+    C* col0 = reinterpret_cast<C*>(bz + (OP == OP_DRIFT ? N + s.nbuf * kTmaMaxTX : 0));
+    // drift: address of A(nx, ny) of column j of tile `id` in the per-grid table
+    auto a_of_tile = [&](long id, int j) {
+        const int ox = (int)(id / s.tiles_x);
+        return s.axy + (s.la3d ? (long)(ox % N) * N : 0L) + (id % s.tiles_x) * TX + j;
+    };
 
     auto coords = [&](long id, int j, int& c0, int& c1, int& c2) {
         const int x0 = (int)(id % s.tiles_x) * TX;
@@ -234,11 +247,9 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         if constexpr (DF) tws_lo[i] = s.tw_lo[i];
     }
     if constexpr (OP == OP_DRIFT) {
-        for (int i = tid; i < N; i += nthr) {
-            const long n = signed_mode(i, N);
-            const double2 w = cis_d(s.phase_fac * (double)(n * n));
-            bz[i] = make_double2(w.x * s.scale, w.y * s.scale);
-        }
+        const double2* gbz = s.axy + (s.la3d ? (long)N * N : (long)N);
+        for (int i = tid; i < N; i += nthr) bz[i] = gbz[i];
+        if (tid < TX && blockIdx.x < s.n_tiles) aslot[tid] = *a_of_tile(blockIdx.x, tid);
     }
     if (tid == 0) {
         s_abort = 0;
@@ -267,6 +278,15 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         const int o = (int)(id / s.tiles_x);
         const int xb = x0 + PW * c;  // column of pencil 0 of this thread
         TileAcc<P, SWZ> acc{reinterpret_cast<P*>(tile), c, TG};
+        // drift: the next tile's A(nx, ny) is copied into its ring slot now
+        // (asynchronously, no registers held) and waited for before this
+        // tile's store barrier, so its latency stays hidden
+        const long id_next = id + gridDim.x;
+        const bool a_copy = OP == OP_DRIFT && tid < TX && id_next < s.n_tiles;
+        if (a_copy) {
+            cp_async16(&aslot[((k + 1) % s.nbuf) * kTmaMaxTX + tid], a_of_tile(id_next, tid));
+            cp_async_commit();
+        }
         P v[E];
         if constexpr (OP == OP_INV) {
 #pragma unroll
@@ -303,14 +323,16 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
             const bool has_col0 = x0 == 0 && c == 0;
             const bool c0ext = (OP == OP_POISSON) && s.col0_external && has_col0;
             if constexpr (OP == OP_DRIFT) {
-                double2 A[PW];
+                // A(nx, ny) of the thread's columns from the tile's ring slot
+                // (staged before the previous tile's store barrier; a multi-stage
+                // forward transform has synchronised the block since)
+                if constexpr (qx_nstages(N) == 1) __syncthreads();
 #pragma unroll
-                for (int h = 0; h < PW; ++h) A[h] = cis_d(s.phase_fac * (double)mxy_of(h));
+                for (int h = 0; h < PW; ++h) {
+                    const double2 A = aslot[b * kTmaMaxTX + PW * c + h];
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    const double2 bze = bz[out_pos<N, E>(e, t)];
-#pragma unroll
-                    for (int h = 0; h < PW; ++h) pen(v[e], h) = cmul_d(pen(v[e], h), dcmul(A[h], bze));
+                    for (int e = 0; e < E; ++e)
+                        pen(v[e], h) = cmul_d(pen(v[e], h), dcmul(A, bz[out_pos<N, E>(e, t)]));
                 }
             } else {
                 SArgs<R> sa;
@@ -364,6 +386,7 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
             }
         }
 
+        if (a_copy) cp_async_wait_all();
         if (store) {
             // finished tile -> buffer (natural order) -> tensor store
             __syncthreads();

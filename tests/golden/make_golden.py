@@ -35,10 +35,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from oracle import REFERENCE_DIR  # noqa: E402
 from oracle import ref_lib as R  # noqa: E402
 from oracle import sp_oracle as O  # noqa: E402
 
-REF_SOLITONS = "/root/reference/solitons.txt"
+REF_SOLITONS = os.path.join(REFERENCE_DIR, "solitons.txt")
 
 
 def make_mre():

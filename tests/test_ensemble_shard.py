@@ -1,6 +1,8 @@
 """Instance sharding of an ensemble over ranks (no collective in the data
 path): a world-size-2 gloo run checks that the ranks' shares cover every box
-exactly once and that each rank gets a near-equal share of every size."""
+exactly once, that each rank gets a near-equal share of every size, and that
+every box is seeded by its global index on whichever rank runs it (the union
+of the ranks' seeds is seed_base + b for every box b, with no duplicates)."""
 import os
 import socket
 
@@ -13,10 +15,14 @@ import torch.multiprocessing as mp  # noqa: E402
 GROUPS = [(64, 16), (96, 16), (128, 16)]
 
 
+SEED_BASE = 1234
+
+
 def _shard(groups, world, rank):
-    # same rule as qaxions_b200.shard_groups, imported lazily in the children
-    from qaxions_b200 import shard_groups
-    return shard_groups(groups, world, rank)
+    # qaxions_b200.shard_groups / shard_seeds, imported lazily in the children
+    from qaxions_b200 import shard_groups, shard_seeds
+    g, mine = shard_groups(groups, world, rank)
+    return g, mine, shard_seeds(groups, world, rank, SEED_BASE)
 
 
 def _worker(rank, world, port, out):
@@ -24,9 +30,8 @@ def _worker(rank, world, port, out):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        groups, mine = _shard(GROUPS, world, rank)
         got = [None] * world
-        dist.all_gather_object(got, (groups, mine))
+        dist.all_gather_object(got, _shard(GROUPS, world, rank))
         if rank == 0:
             out.put(got)
     finally:
@@ -48,9 +53,29 @@ def test_shard_groups_gloo_world2():
     world = 2
     mp.start_processes(_worker, args=(world, _free_port(), q), nprocs=world, join=True, start_method="spawn")
     got = q.get()
-    all_boxes = sorted(b for _, mine in got for b in mine)
-    assert all_boxes == list(range(sum(c for _, c in GROUPS)))
-    for groups, mine in got:
-        assert sum(c for _, c in groups) == len(mine)
+    all_boxes = sorted(b for _, mine, _ in got for b in mine)
+    nbox = sum(c for _, c in GROUPS)
+    assert all_boxes == list(range(nbox))
+    all_seeds = [x for _, _, seeds in got for x in seeds]
+    assert sorted(all_seeds) == [SEED_BASE + b for b in range(nbox)]  # no duplicates, none missing
+    size_of = [n for n, c in GROUPS for _ in range(c)]
+    for groups, mine, seeds in got:
+        assert sum(c for _, c in groups) == len(mine) == len(seeds)
         for n, c in groups:
             assert c == 8  # 16 boxes of each size split evenly over 2 ranks
+        # local box i (numbered group by group, as Ensemble does) is global box mine[i]
+        local_sizes = [n for n, c in groups for _ in range(c)]
+        assert local_sizes == [size_of[b] for b in mine]
+        assert seeds == [SEED_BASE + b for b in mine]
+
+
+def test_shard_groups_repeated_sizes():
+    from qaxions_b200 import shard_groups
+    groups = [(64, 3), (96, 2), (64, 4)]
+    size_of = [n for n, c in groups for _ in range(c)]
+    seen = []
+    for rank in range(3):
+        g, mine = shard_groups(groups, 3, rank)
+        assert [n for n, c in g for _ in range(c)] == [size_of[b] for b in mine]
+        seen += mine
+    assert sorted(seen) == list(range(9))

@@ -13,9 +13,10 @@ import os
 import numpy as np
 import pytest
 
+import pyqaxions.fieldtest as fieldtest  # the reference tests' own import (tests/test_field.py:8)
+import pyqaxions.ictest as ictest  # (tests/test_ic.py:8)
 import qaxions_b200 as qx
 from oracle import sp_oracle as O
-from qaxions_b200.pyqaxions import fieldtest, ictest
 
 pytestmark = pytest.mark.gpu
 
@@ -55,7 +56,10 @@ def _call_pin(kind, n, N, dt, idx, dtype):
 @pytest.mark.parametrize("dtype", ["c128", "c64"])
 def test_reference_test_surface(soliton_dir, dtype):
     """The reference's own pybind test functions, same arguments, same values
-    (tests/test_field.py:12-129, tests/test_ic.py:12-37)."""
+    (tests/test_field.py:12-129, tests/test_ic.py:12-37): the pybind11 modules
+    pyqaxions.fieldtest / pyqaxions.ictest of this library, imported under the
+    reference's names, at every grid point of the reference's tests, against
+    the values the reference's own modules return (tests/golden/golden_pins.npz)."""
     for kind, n, N, dt, idx, val in zip(PINS["kind"], PINS["dim"], PINS["N"], PINS["dt"], PINS["idx"],
                                         PINS["value"]):
         got = _call_pin(str(kind), int(n), int(N), float(dt), int(idx), dtype)
@@ -312,13 +316,19 @@ def test_tma_and_direct_strided_kernels_agree(dim, N, dtype):
 
 def test_fp32_kick_accuracy():
     """The FP32 kick psi exp(-i dt V) against FP64 on the same FP32 inputs, for
-    phases across many quadrants and for small phases."""
+    phases across many quadrants and for small phases.  dt = 0.37 dx^2 is not
+    representable in FP32, so the phase dt V must be formed and reduced mod
+    2 pi in FP64 (an FP32 product would be off by up to |dt V| 6e-8, 3.6e-6 at
+    |dt V| = 60); the bound is the FP32 rounding of the reduced phase, of
+    sincosf's result and of the complex product."""
     rng = np.random.default_rng(7)
     N = 32
     f = qx.Field(3, N, dtype="c64")
     shape = f.shape
     psi = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(np.complex64).astype(np.complex128)
-    for dt, vmax in ((1.0, 60.0), (1.0, 3.0), (1e-3, 0.05)):
+    dt37 = 0.37 / N**2
+    for dt, vmax in ((1.0, 60.0), (1.0, 3.0), (1e-3, 0.05), (dt37, 60.0 / dt37), (dt37, 3.0 / dt37),
+                     (dt37, 1e-3 / dt37)):
         V = (rng.uniform(-vmax, vmax, size=shape)).astype(np.float32).astype(np.float64)
         f.psi = psi
         f.V = V
