@@ -576,7 +576,7 @@ class FieldT final : public Field {
             for (int i = 0; i < nsteps - 1; ++i) {
                 if (graph_enabled_) {
                     if (!graph_exec_ || graph_dt_ != ds_) capture_body();
-                    QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
+                    launch_graph();
                 } else {
                     body(ds_, ds_, pref_eff(), false);
                 }
@@ -730,7 +730,7 @@ class FieldT final : public Field {
                 } else {
                     if (!last && graph_enabled_) {
                         if (!graph_exec_ || graph_dt_ != ds_) capture_body();
-                        QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
+                        launch_graph();
                     } else {
                         body(ds_, ds_, pref_eff(), last);
                     }
@@ -764,6 +764,13 @@ class FieldT final : public Field {
         v_current_ = !(last_measured && (mask & MEAS_CLOBBER_V));
         vmax_stale_ = true;
         QX_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    // replay the captured loop body; its drift pass reads the factor tables
+    // of ds_, which an eager pass with another time step may have replaced
+    void launch_graph() {
+        ensure_axy(ds_);
+        QX_CUDA(cudaGraphLaunch(graph_exec_, st_));
     }
 
     void capture_body() {

@@ -116,17 +116,40 @@ template <typename C> __device__ __forceinline__ C cmul_d(C v, double2 w) {
     return mk<C>((decltype(C::x))fma(vx, w.x, -vy * w.y), (decltype(C::x))fma(vx, w.y, vy * w.x));
 }
 
+// exp(i phi) for the FP32 kick.  phi (FP64) is reduced in FP64 to
+// r in [-pi/4, pi/4] and a quadrant q (Cody-Waite reduction with pi/2 split
+// into its double and the remainder), r is rounded once to FP32, and sin r,
+// cos r come from polynomials in r^2 fitted on that interval
+// (fit_kick_poly.py: largest error 4.7e-8 for sin, 6.5e-8 for cos), then
+// rotated by i^q.
+__device__ __forceinline__ float2 cis_kick(double phi) {
+    const double two_over_pi = 0.636619772367581343075535053490057448;
+    const double pio2_hi = 1.57079632679489655800;   // the double nearest pi/2
+    const double pio2_lo = 6.12323399573676588613e-17;  // pi/2 - pio2_hi
+    const double qd = rint(phi * two_over_pi);
+    const int k = (int)(__double2ll_rn(qd) & 3);
+    const float r = (float)fma(-qd, pio2_lo, fma(-qd, pio2_hi, phi));
+    const float r2 = r * r;
+    const float sn = fmaf(r * r2, fmaf(r2, fmaf(r2, -0x1.9aca00p-13f, 0x1.110c2ap-7f), -0x1.555552p-3f), r);
+    const float cs =
+        fmaf(r2, fmaf(r2, fmaf(r2, fmaf(r2, 0x1.9a6fb4p-16f, -0x1.6c0e0ap-10f), 0x1.55554cp-5f), -0.5f), 1.0f);
+    float re = (k & 1) ? sn : cs, im = (k & 1) ? cs : sn;
+    if ((k + 1) & 2) re = -re;  // k = 1, 2
+    if (k & 2) im = -im;        // k = 2, 3
+    return make_float2(re, im);
+}
+
 // psi * exp(-i dt V)   (src/field.cxx:100-112).  Both forms form the phase
-// -dt V in FP64 and reduce it mod 2 pi there; the FP32 form then rounds the
-// reduced phase (|phi| <= pi) once and takes sincosf of it.  Forming dt V in
-// FP32 instead would round dt itself (a fixed relative error applied at
-// every step) and lose |dt V| 6e-8 of absolute phase to the product.
+// -dt V in FP64 and reduce it there (FP64: mod 2 pi, then sincos; FP32: to
+// [-pi/4, pi/4] and a quadrant, cis_kick).  Forming dt V in FP32 instead
+// would round dt itself (a fixed relative error applied at every step) and
+// lose |dt V| 6e-8 of absolute phase to the product.
 template <typename R> __device__ __forceinline__ cx_t<R> kick1(cx_t<R> p, R v, double dt);
 template <> __device__ __forceinline__ double2 kick1<double>(double2 p, double v, double dt) {
     return cmul(p, cis<double>(-dt * v));
 }
 template <> __device__ __forceinline__ float2 kick1<float>(float2 p, float v, double dt) {
-    return cmul(p, cis<float>(-dt * (double)v));
+    return cmul(p, cis_kick(-dt * (double)v));
 }
 
 __device__ __forceinline__ int signed_mode(int i, int N) { return i <= (N >> 1) ? i : i - N; }

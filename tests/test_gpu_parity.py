@@ -356,3 +356,21 @@ def test_mre_cosmology_matches_reference(dtype):
         err = O.rel_l2(f.psi, d[f"{tag}_psi_run"])
         assert err <= (1e-12 if dtype == "c128" else 1e-5), (tag, err)
         f.close()
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_graph_replay_after_eager_drift_with_another_dt(dtype):
+    """The captured loop body reads the drift factor tables of its time step;
+    an eager drift with another step replaces them, and the next replay must
+    see its own again: graph replays equal the same sequence run eagerly."""
+    N = 32
+    dt = 0.2 / N**2
+    outs = []
+    for use_graph in (True, False):
+        with qx.Field(3, N, pref=1.0, dtype=dtype, dt=dt) as f:
+            f.ic_config(qx.IC_GRF, 12, 2, 0.05, 0.1)
+            f.time_steps(4, use_graph)
+            f.drift(3.7 * dt)
+            f.time_steps(4, use_graph)
+            outs.append(f.psi)
+    assert np.array_equal(outs[0], outs[1])
