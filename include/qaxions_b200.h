@@ -177,12 +177,6 @@ int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, dou
  * 0 = direct loads; -1 = keep), TMA ring depth, pencils per thread of the TMA
  * passes (1 or 2; 0 = default: 2 in the FP32 form, FP64 always 1) */
 int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw);
-/* FFT exchange scheme of the FP32 paired-pencil strided passes at N = 256 and
- * 512 (no counterpart in the reference, whose FFTs are FFTW's): 0 (default)
- * two block barriers per stage exchange in the tile buffer, 3-deep TMA ring;
- * 1 exchanges alternating between the tile and a scratch tile, one barrier
- * each, 2-deep ring.  Results are bit-identical. */
-int qx_set_exchange(qx_field_t *h, int pingpong);
 /* Drift chain (no counterpart in the reference: the reference's drift,
  * src/field.cxx:119-198, is three library FFT calls around a multiply).  on = 0
  * (default): the y forward, z drift and y inverse passes of a 3D complex64

@@ -94,7 +94,6 @@ _SIGS = {
     "qx_profile_step": ([_vp, _i, _i, C.c_char_p, _dp, _ip], _i),
     "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
     "qx_set_chain": ([_vp, _i], _i),
-    "qx_set_exchange": ([_vp, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
     "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
@@ -416,12 +415,6 @@ class Field:
         persistent or the direct-load strided kernels (-1 keeps the current);
         pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
         self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
-
-    def set_exchange(self, pingpong: bool):
-        """FFT exchanges of the FP32 strided passes at N = 256, 512: in the tile
-        (False, default) or ping-pong through a scratch tile (True); the
-        results are bit-identical."""
-        self._c("qx_set_exchange", int(bool(pingpong)))
 
     def set_chain(self, on):
         """Drift chain: the y, z-drift, y passes of a 3D complex64 field as

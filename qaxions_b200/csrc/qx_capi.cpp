@@ -279,14 +279,6 @@ int qx_set_tune(qx_field_t* h, int x_rows, int y_tx, int la_tx, int tma, int nbu
     });
 }
 
-int qx_set_exchange(qx_field_t* h, int pingpong) {
-    return guarded(h, [&](qx::Field& f) {
-        need(pingpong == 0 || pingpong == 1, "pingpong must be 0 or 1");
-        f.tune().pp = pingpong;
-        f.invalidate_graph();
-    });
-}
-
 int qx_set_chain(qx_field_t* h, int on) {
     return guarded(h, [&](qx::Field& f) {
         need(on >= 0 && on <= 2, "chain must be 0, 1 or 2");

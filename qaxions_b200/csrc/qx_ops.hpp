@@ -23,8 +23,6 @@ struct Tune {
     int pw = 0;       // pencils per thread of TMA passes (0 = default: 2 in FP32, 1 in FP64)
     int chain = 0;    // FP32 3D drift's y / z / y passes: 0 three passes; 1 / 2 one slab-ordered
                       // kernel over slabs of `chain` 8-column tiles (bit-identical, measured slower)
-    int pp = 0;       // FP32 paired-pencil 8-column strided passes (N = 256, 512): FFT exchanges
-                      // ping-pong through a scratch tile (one barrier each; 2-deep ring)
 };
 
 template <typename R> struct Ops {

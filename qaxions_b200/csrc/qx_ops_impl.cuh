@@ -282,12 +282,10 @@ template <typename R, int OP> static bool use_df(const typename Ops<R>::SP& a) {
 }
 
 // Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
-// PP: ping-pong exchanges (one scratch tile, a 2-deep ring).
-template <int NN, typename R, int OP, int PW, bool DF, int TXF, bool PP = false>
+template <int NN, typename R, int OP, int PW, bool DF, int TXF>
 static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                          const Tune& tu, cudaStream_t st) {
-    TmaGeom g = tma_geom<NN, R, PW, TXF>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
-    if (PP) g.nbuf = 2;  // ring + scratch of two blocks per SM
+    const TmaGeom g = tma_geom<NN, R, PW, TXF>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
     TArgs<R> s;
     s.tw = a.tw;
     s.tw_lo = a.tw_lo;
@@ -313,8 +311,8 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.err = a.err;
     constexpr bool SWZ = tma_swizzled<NN, R, PW, TXF>();
     const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim, SWZ);
-    auto kern = k_pencil_tma<NN, R, OP, PW, DF, TXF, PP>;
-    const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf + (PP ? 1 : 0), OP, SWZ);
+    auto kern = k_pencil_tma<NN, R, OP, PW, DF, TXF>;
+    const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP, SWZ);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
     const int key = g.nbuf * 8 + (g.TX == 16 ? 4 : g.TX == 8 ? 3 : g.TX == 4 ? 2 : g.TX == 2 ? 1 : 0);
@@ -345,9 +343,6 @@ static long launch_tma_tx(const typename Ops<R>::SP& a, int NZ, int outer, int p
         const int tx = want == 8 || want == 16 ? want : 8;
         if constexpr (sizeof(R) == 4 && NN >= 64) {
             if (tx == 16) return launch_tma_e<NN, R, OP, PW, DF, 16>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
-        }
-        if constexpr (sizeof(R) == 4 && PW == 2 && (NN == 256 || NN == 512)) {
-            if (tu.pp) return launch_tma_e<NN, R, OP, PW, DF, 8, true>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
         }
         return launch_tma_e<NN, R, OP, PW, DF, 8>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
     }

@@ -188,44 +188,10 @@ template <typename P, bool SWZ> struct TileAcc {
     }
 };
 
-// Ping-pong exchanges: the FFT stages alternate between the tile buffer and
-// a scratch buffer of the same layout, so each exchange needs one block
-// barrier (after its writes) instead of two: a buffer is written again only
-// after a later exchange's barrier, which every thread passes after its last
-// read of that buffer.  Calls of sync() come in pairs per exchange (before
-// the writes, before the reads): the first switches buffers, the second is
-// the barrier.  Element access and layout are those of TileAcc (plain).
-template <typename P> struct PingPongAcc {
-    P* base[2];
-    int c, pitch;
-    int cur = 0, n = 0;
-    __device__ __forceinline__ P& operator()(int p) const { return base[cur][p * pitch + c]; }
-    __device__ __forceinline__ void sync() {
-        if ((n++ & 1) == 0) cur ^= 1;
-        else __syncthreads();
-    }
-};
-
-template <typename Acc, typename P, bool SWZ>
-__device__ __forceinline__ Acc make_acc(const TileAcc<P, SWZ>& tile, P* scratch) {
-    if constexpr (std::is_same<Acc, TileAcc<P, SWZ>>::value) {
-        (void)scratch;
-        return tile;
-    } else {
-        Acc a;
-        a.base[0] = tile.base;
-        a.base[1] = scratch;
-        a.c = tile.c;
-        a.pitch = tile.pitch;
-        return a;
-    }
-}
-
 // blockDim = (TX / PW, N / E, 1), or (TX / PW / 2, N / E, 2) when swizzled:
 // thread (c, t) owns columns x0 + PW c + h (h < PW), c = x + blockDim.x z;
-// TX = TXF when TXF > 0.  PP: ping-pong exchanges through one scratch tile
-// (kept after the ring; not with the swizzled layout).
-template <int N, typename R, int OP, int PW, bool DF, int TXF, bool PP = false>
+// TX = TXF when TXF > 0
+template <int N, typename R, int OP, int PW, bool DF, int TXF>
 __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_block_min<N, R, PW, TXF>()))
     k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
@@ -246,10 +212,8 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
     const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
     // tiles on 128-byte boundaries, 1024 for the 128-byte swizzle
     constexpr uintptr_t BA = SWZ ? 1023 : 127;
-    static_assert(!(PP && SWZ), "ping-pong exchanges use the plain tile layout");
     C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + BA) & ~BA);
-    C* scratch = bufs + s.nbuf * tile_elems;  // PP only
-    C* tws = bufs + (s.nbuf + (PP ? 1 : 0)) * tile_elems;
+    C* tws = bufs + s.nbuf * tile_elems;
     C* tws_lo = tws + N;
     double2* bz = reinterpret_cast<double2*>(tws_lo + N);
     double2* aslot = bz + N;  // drift: A(nx, ny) of each ring buffer's tile columns
@@ -314,9 +278,7 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         const int x0 = (int)(id % s.tiles_x) * TX;
         const int o = (int)(id / s.tiles_x);
         const int xb = x0 + PW * c;  // column of pencil 0 of this thread
-        TileAcc<P, SWZ> tacc{reinterpret_cast<P*>(tile), c, TG};
-        using Acc = typename std::conditional<PP, PingPongAcc<P>, TileAcc<P, SWZ>>::type;
-        Acc acc = make_acc<Acc>(tacc, reinterpret_cast<P*>(scratch));
+        TileAcc<P, SWZ> acc{reinterpret_cast<P*>(tile), c, TG};
         // drift: the next tile's A(nx, ny) is copied into its ring slot now
         // (asynchronously, no registers held) and waited for before this
         // tile's store barrier, so its latency stays hidden
@@ -432,10 +394,10 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
             __syncthreads();
             if constexpr (OP == OP_FWD) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) tacc(out_pos<N, E>(e, t)) = v[e];
+                for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
             } else {
 #pragma unroll
-                for (int e = 0; e < E; ++e) tacc(in_pos<N, E, 0>(e, t)) = v[e];
+                for (int e = 0; e < E; ++e) acc(in_pos<N, E, 0>(e, t)) = v[e];
             }
             fence_proxy_async();
             __syncthreads();
