@@ -177,6 +177,16 @@ int qx_profile_step(qx_field_t *h, int nsteps, int max_entries, char *names, dou
  * 0 = direct loads; -1 = keep), TMA ring depth, pencils per thread of the TMA
  * passes (1 or 2; 0 = default: 2 in the FP32 form, FP64 always 1) */
 int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbuf, int pw);
+/* Radix plan of the TMA strided (y / last-axis) passes, no counterpart in the
+ * reference (FFTW plans its own): 0 default, 1 the same radices in reverse
+ * order, for grids whose default plan mixes radix sizes (N = 64, 96, 128,
+ * 256); elsewhere plan 1 runs as plan 0.  Results agree to round-off. */
+int qx_set_plan(qx_field_t *h, int plan);
+/* the launch geometry in use: out[9] = {x_rows, y_tx, la_tx, tma, nbuf, pw,
+ * plan, chain, from_cache}; from_cache = 1 when the field took it from the
+ * autotuner's cache at creation (the process cache, or the file named by the
+ * environment variable QX_TUNE_CACHE) */
+int qx_get_tune(qx_field_t *h, int *out, int n);
 /* Drift chain (no counterpart in the reference: the reference's drift,
  * src/field.cxx:119-198, is three library FFT calls around a multiply).  on = 0
  * (default): the y forward, z drift and y inverse passes of a 3D complex64
@@ -186,12 +196,16 @@ int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbu
  * in all three modes; on B200 the three passes are faster at every size
  * measured (64^3 .. 512^3). */
 int qx_set_chain(qx_field_t *h, int on);
-/* Autotuner: time nsteps steps under each candidate launch geometry (pencils
- * per thread, TMA ring depth, tile widths, rows per x block), keep the fastest;
- * psi is restored afterwards.  Cached per (dim, N, dtype, batch) in the process
- * and in the text file cache_path if not NULL (read first, appended after).
- * best_ms: ms per step of the choice; from_cache: 1 if nothing was timed. */
+/* Autotuner: time nsteps steps under each candidate launch geometry (radix
+ * plan of the strided passes, pencils per thread, TMA ring depth, tile widths,
+ * rows per x block), keep the fastest; psi is restored afterwards.  Cached per
+ * (dim, N, dtype, batch) in the process and in the text file cache_path if not
+ * NULL (read first, appended after); fields created later with the same key
+ * start with the cached geometry (qx_get_tune).  best_ms: ms per step of the
+ * choice; from_cache: 1 if nothing was timed. */
 int qx_autotune(qx_field_t *h, int nsteps, const char *cache_path, double *best_ms, int *from_cache);
+/* forget the autotuner's in-process choices (cache files are not touched) */
+int qx_clear_tune_cache(void);
 int qx_device_pointers(qx_field_t *h, void **psi, void **V);
 /* dst psi <- src psi on the device (same dim, N, batch and dtype) */
 int qx_copy_psi(qx_field_t *dst, qx_field_t *src);

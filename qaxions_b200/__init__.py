@@ -94,6 +94,9 @@ _SIGS = {
     "qx_profile_step": ([_vp, _i, _i, C.c_char_p, _dp, _ip], _i),
     "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
     "qx_set_chain": ([_vp, _i], _i),
+    "qx_set_plan": ([_vp, _i], _i),
+    "qx_clear_tune_cache": ([], _i),
+    "qx_get_tune": ([_vp, _ip, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
     "qx_sync": ([_vp], _i),
     "qx_autotune": ([_vp, _i, C.c_char_p, _dp, _ip], _i),
@@ -154,6 +157,11 @@ def meas_list(nsteps: int, nmeas: int):
     n = C.c_int()
     _check(_lib.qx_meas_list(int(nsteps), int(nmeas), out, max(int(nmeas), 1), C.byref(n)))
     return [int(out[i]) for i in range(n.value)]
+
+
+def clear_tune_cache():
+    """Forget the autotuner's in-process choices (cache files are left alone)."""
+    _check(_lib.qx_clear_tune_cache())
 
 
 def set_device(device: int):
@@ -415,6 +423,19 @@ class Field:
         persistent or the direct-load strided kernels (-1 keeps the current);
         pw: pencils per thread of the TMA passes (0 default, 1 or 2)."""
         self._c("qx_set_tune", x_rows, y_tx, la_tx, tma, nbuf, pw)
+
+    def set_plan(self, plan: int):
+        """Radix plan of the strided passes: 0 default, 1 reversed radix order
+        (grids N = 64, 96, 128, 256; elsewhere it runs as 0)."""
+        self._c("qx_set_plan", int(plan))
+
+    def get_tune(self) -> dict:
+        """The launch geometry in use (and whether it came from the autotuner's
+        cache when the field was created)."""
+        v = (C.c_int * 9)()
+        self._c("qx_get_tune", v, 9)
+        keys = ("x_rows", "y_tx", "la_tx", "tma", "nbuf", "pw", "plan", "chain", "from_cache")
+        return dict(zip(keys, list(v)))
 
     def set_chain(self, on):
         """Drift chain: the y, z-drift, y passes of a 3D complex64 field as

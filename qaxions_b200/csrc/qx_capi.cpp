@@ -279,6 +279,28 @@ int qx_set_tune(qx_field_t* h, int x_rows, int y_tx, int la_tx, int tma, int nbu
     });
 }
 
+int qx_clear_tune_cache(void) {
+    qx::clear_tune_cache();
+    return QX_OK;
+}
+
+int qx_set_plan(qx_field_t* h, int plan) {
+    return guarded(h, [&](qx::Field& f) {
+        need(plan == 0 || plan == 1, "plan must be 0 or 1");
+        f.tune().plan = plan;
+        f.invalidate_graph();
+    });
+}
+
+int qx_get_tune(qx_field_t* h, int* out, int n) {
+    return guarded(h, [&](qx::Field& f) {
+        need(out && n >= 9, "out must hold 9 ints");
+        const qx::Tune& t = f.tune();
+        const int v[9] = {t.x_rows, t.y_tx, t.la_tx, t.tma, t.nbuf, t.pw, t.plan, t.chain, f.tuned_from_cache() ? 1 : 0};
+        for (int i = 0; i < 9; ++i) out[i] = v[i];
+    });
+}
+
 int qx_set_chain(qx_field_t* h, int on) {
     return guarded(h, [&](qx::Field& f) {
         need(on >= 0 && on <= 2, "chain must be 0, 1 or 2");

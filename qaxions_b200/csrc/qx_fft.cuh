@@ -74,33 +74,55 @@ template <typename C> __device__ __forceinline__ C& pen(C& v, int) { return v; }
 template <typename C> __device__ __forceinline__ C& pen(CPair<C>& v, int h) { return h ? v.b : v.a; }
 
 // ---------------------------------------------------------------------------
-// Radix plans (compile time).  L = 2^e: [8]*(e/3) + [2^(e%3) if e%3] (e <= 3:
-// one stage of radix L) -- the radix-8 stages come first so that every
-// shared-memory exchange of a one-warp-per-row transform is bank-conflict free
-// under RowAcc's padding.  L = 3*2^k: [4]*(k/2) + [2]*(k%2) + [3].
+// Radix plans (compile time).  Default plan of a length n: n = 2^e:
+// [8]*(e/3) + [2^(e%3) if e%3] (e <= 3: one stage of radix n) -- the radix-8
+// stages come first so that every shared-memory exchange of a one-warp-per-row
+// transform is bank-conflict free under RowAcc's padding.  n = 3*2^k:
+// [4]*(k/2) + [2]*(k%2) + [3].
+//
+// A transform length L may carry a plan index in its high bits,
+// L = n | (plan << 16) (qx_with_plan): plan 0 is the default order above, plan
+// 1 the same radices in reverse order (same elements per thread, other stage
+// spans, twiddles and exchange patterns; the strided passes offer it to the
+// autotuner).  Everything below takes such an L; qx_len(L) is the length.
 // ---------------------------------------------------------------------------
 
-__host__ __device__ constexpr bool qx_is_pow2(int L) { return L > 0 && (L & (L - 1)) == 0; }
-__host__ __device__ constexpr int qx_log2(int L) { return L <= 1 ? 0 : 1 + qx_log2(L / 2); }
+__host__ __device__ constexpr int qx_len(int L) { return L & 0xFFFF; }
+__host__ __device__ constexpr int qx_plan(int L) { return L >> 16; }
+__host__ __device__ constexpr int qx_with_plan(int n, int plan) { return n | (plan << 16); }
 
-__host__ __device__ constexpr int qx_nstages(int L) {
-    return qx_is_pow2(L) ? (qx_log2(L) <= 3 ? 1 : (qx_log2(L) / 3 + (qx_log2(L) % 3 ? 1 : 0)))
-                         : (qx_log2(L / 3) / 2 + qx_log2(L / 3) % 2 + 1);
+__host__ __device__ constexpr bool qx_is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+__host__ __device__ constexpr int qx_log2(int n) { return n <= 1 ? 0 : 1 + qx_log2(n / 2); }
+
+__host__ __device__ constexpr int qx_nstages0(int n) {
+    return qx_is_pow2(n) ? (qx_log2(n) <= 3 ? 1 : (qx_log2(n) / 3 + (qx_log2(n) % 3 ? 1 : 0)))
+                         : (qx_log2(n / 3) / 2 + qx_log2(n / 3) % 2 + 1);
 }
+__host__ __device__ constexpr int qx_nstages(int L) { return qx_nstages0(qx_len(L)); }
 
-__host__ __device__ constexpr int qx_radix(int L, int s) {
-    if (qx_is_pow2(L)) {
-        const int e = qx_log2(L);
-        if (e <= 3) return L;
+// radix of stage s of the default plan of length n
+__host__ __device__ constexpr int qx_radix0(int n, int s) {
+    if (qx_is_pow2(n)) {
+        const int e = qx_log2(n);
+        if (e <= 3) return n;
         const int rem = e % 3;
         if (rem) return s == e / 3 ? (1 << rem) : 8;
         return 8;
     }
-    const int k = qx_log2(L / 3);
+    const int k = qx_log2(n / 3);
     const int n4 = k / 2, n2 = k % 2;
     if (s < n4) return 4;
     if (s < n4 + n2) return 2;
     return 3;
+}
+
+__host__ __device__ constexpr int qx_radix(int L, int s) {
+    return qx_radix0(qx_len(L), qx_plan(L) == 1 ? qx_nstages(L) - 1 - s : s);
+}
+
+// does plan 1 differ from plan 0 for length n (radices not all equal)?
+__host__ __device__ constexpr bool qx_plan1_differs(int n, int s = 1) {
+    return s >= qx_nstages0(n) ? false : (qx_radix0(n, s) != qx_radix0(n, 0) || qx_plan1_differs(n, s + 1));
 }
 
 __host__ __device__ constexpr int qx_span(int L, int s) {  // product of radices before stage s
@@ -205,7 +227,7 @@ template <int r, int SIGN, typename C> __device__ __forceinline__ void dft(C* a)
 // transform of length L/2 leaves its real output and a c2r transform takes
 // its real input, so a row pass can chain them without a shared-memory copy.
 template <int L, int E, int s, int J0> __device__ __forceinline__ int stage_j(int b, int t) {
-    constexpr int T = L / E;
+    constexpr int T = qx_len(L) / E;
     if constexpr (s == 0 && J0 == 1) {
         static_assert((E / qx_radix(L, 0)) % 2 == 0, "paired stage-0 columns need an even number of blocks");
         return 2 * t + 2 * T * (b >> 1) + (b & 1);
@@ -217,13 +239,13 @@ template <int L, int E, int s, int J0> __device__ __forceinline__ int stage_j(in
 // position held in v[e] before stage s (stage-s input order)
 template <int L, int E, int s, int J0 = 0> __device__ __forceinline__ int in_pos(int e, int t) {
     constexpr int r = qx_radix(L, s);
-    return stage_j<L, E, s, J0>(e / r, t) + (e % r) * (L / r);
+    return stage_j<L, E, s, J0>(e / r, t) + (e % r) * (qx_len(L) / r);
 }
 // position held in v[e] after the last stage (natural-order output)
 template <int L, int E> __device__ __forceinline__ int out_pos(int e, int t) {
     constexpr int r = qx_radix(L, qx_nstages(L) - 1);
-    constexpr int T = L / E;
-    return t + (e / r) * T + (e % r) * (L / r);
+    constexpr int T = qx_len(L) / E;
+    return t + (e / r) * T + (e % r) * (qx_len(L) / r);
 }
 
 // Twiddle tables are stage-major: stage s >= 1 (span Ns, radix r) keeps its

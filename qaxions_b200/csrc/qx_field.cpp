@@ -2,6 +2,7 @@
 #include "qx_field.hpp"
 
 #include <cmath>
+#include <cstdlib>
 #include <limits>
 #include <cstring>
 #include <fstream>
@@ -218,14 +219,16 @@ static typename Ops<R>::XP xp0(const Geometry& g, const TwTables<typename Ops<R>
 
 template <typename R>
 static typename Ops<R>::SP sp0(int* err, const Geometry& g, typename Ops<R>::C* a,
-                               const TwTables<typename Ops<R>::C>& tw, int X) {
+                               const TwTables<typename Ops<R>::C>& tw, int X, const Tune& tu) {
     typename Ops<R>::SP s{};
     s.err = err;
     s.a = a;
-    s.tw = tw.N;
+    // radix plan 1 where the TMA passes run and the grid has it
+    s.plan = (tu.tma && tu.plan == 1 && tw.N_p1) ? 1 : 0;
+    s.tw = s.plan ? tw.N_p1 : tw.N;
     // double-float twiddles for wave-function arrays (X = N) only: the
     // half-spectrum (density / potential) transforms keep single twiddles
-    s.tw_lo = X == g.N ? tw.N_lo : nullptr;
+    s.tw_lo = X == g.N ? (s.plan ? tw.N_p1_lo : tw.N_lo) : nullptr;
     s.X = X;
     s.dim = g.dim;
     s.N = g.N;
@@ -240,8 +243,8 @@ template <typename R> void B200FFTBackend<R>::forward_c2c(void* data) {
     a.in = d;
     a.out = d;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,d, tw_, g_.N), -1, *tune_, st_);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, tw_, g_.N), OP_FWD, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_, d, tw_, g_.N, *tune_), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_, d, tw_, g_.N, *tune_), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C* out) {
@@ -249,13 +252,13 @@ template <typename R> void B200FFTBackend<R>::forward_c2c_partial(const C* in, C
     a.in = in;
     a.out = out;
     Ops<R>::x_fwd(g_.N, a, false, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,out, tw_, g_.N), -1, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_, out, tw_, g_.N, *tune_), -1, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2c(void* data) {
     C* d = static_cast<C*>(data);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,d, tw_, g_.N), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,d, tw_, g_.N), +1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_, d, tw_, g_.N, *tune_), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_, d, tw_, g_.N, *tune_), +1, *tune_, st_);
     auto a = xp0<R>(g_, tw_);
     a.in = d;
     a.out = d;
@@ -268,14 +271,14 @@ template <typename R> void B200FFTBackend<R>::forward_r2c(void* in_real, void* o
     a.Vin = static_cast<const R*>(in_real);
     a.vh = h;
     Ops<R>::x_r2c(g_.N, a, true, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), -1, *tune_, st_);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), OP_FWD, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_, h, tw_, g_.N / 2, *tune_), -1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_, h, tw_, g_.N / 2, *tune_), OP_FWD, *tune_, st_);
 }
 
 template <typename R> void B200FFTBackend<R>::backward_c2r(void* in_half, void* out_real) {
     C* h = static_cast<C*>(in_half);
-    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), OP_INV, *tune_, st_);
-    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_,h, tw_, g_.N / 2), +1, *tune_, st_);
+    Ops<R>::la_pass(g_.N, sp0<R>(err_, g_, h, tw_, g_.N / 2, *tune_), OP_INV, *tune_, st_);
+    if (g_.dim == 3) Ops<R>::y_pass(g_.N, g_.B * g_.N, sp0<R>(err_, g_, h, tw_, g_.N / 2, *tune_), +1, *tune_, st_);
     auto a = xp0<R>(g_, tw_);
     a.vh = h;
     a.Vout = static_cast<R*>(out_real);
@@ -331,13 +334,15 @@ void Field::propagate() {  // src/field.cxx:388-402
 }
 
 // ---------------------------------------------------------------------------
-// autotuner cache: "dim N dtype batch : x_rows y_tx la_tx tma nbuf pw ms"
+// autotuner cache: "v2 dim N dtype batch : x_rows y_tx la_tx tma nbuf pw plan ms"
 // ---------------------------------------------------------------------------
 
 static std::map<std::string, std::pair<Tune, double>>& tune_cache() {
     static std::map<std::string, std::pair<Tune, double>> c;
     return c;
 }
+
+void clear_tune_cache() { tune_cache().clear(); }
 
 static bool tune_lookup(const std::string& key, const char* path, Tune& t, double& ms) {
     auto& c = tune_cache();
@@ -351,7 +356,7 @@ static bool tune_lookup(const std::string& key, const char* path, Tune& t, doubl
             std::istringstream vs(line.substr(colon + 3));
             Tune u;
             double m = 0.0;
-            if (vs >> u.x_rows >> u.y_tx >> u.la_tx >> u.tma >> u.nbuf >> u.pw >> m) c[key] = {u, m};
+            if (vs >> u.x_rows >> u.y_tx >> u.la_tx >> u.tma >> u.nbuf >> u.pw >> u.plan >> m) c[key] = {u, m};
         }
         it = c.find(key);
     }
@@ -366,7 +371,7 @@ static void tune_store(const std::string& key, const char* path, const Tune& t, 
     if (path && *path) {
         std::ofstream out(path, std::ios::app);
         out << key << " : " << t.x_rows << " " << t.y_tx << " " << t.la_tx << " " << t.tma << " " << t.nbuf << " "
-            << t.pw << " " << ms << "\n";
+            << t.pw << " " << t.plan << " " << ms << "\n";
     }
 }
 
@@ -418,11 +423,21 @@ class FieldT final : public Field {
         upload(twNl_, sNl);
         upload(twMl_, sMl);
         upload(twNn_, tN);
-        tw_ = TwTables<C>{twN_.as<C>(), twM_.as<C>(), twNl_.as<C>(), twMl_.as<C>(), twNn_.as<C>()};
+        tw_ = TwTables<C>{twN_.as<C>(), twM_.as<C>(), twNl_.as<C>(), twMl_.as<C>(), twNn_.as<C>(), nullptr, nullptr};
+        if (Ops<R>::has_plan1(cfg.N)) {
+            std::vector<C> sP(tN.size(), C{0, 0}), sPl(tN.size(), C{0, 0});
+            Ops<R>::stage_twiddles(tN.data(), plan_tagged(cfg.N, 1), sP.data());
+            Ops<R>::stage_twiddles(tNl.data(), plan_tagged(cfg.N, 1), sPl.data());
+            upload(twP_, sP);
+            upload(twPl_, sPl);
+            tw_.N_p1 = twP_.as<C>();
+            tw_.N_p1_lo = twPl_.as<C>();
+        }
         QX_CUDA(cudaMemsetAsync(psi_.p, 0, psi_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
         fft_ = std::make_unique<B200FFTBackend<R>>(g_, tw_, &tune_, st_, err_);
+        consult_tune_cache();
         // drift chain: phase counters (as many as 8-column slabs need)
         chain_n_ = Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, 1);
         if (chain_n_) chain_.alloc(sizeof(unsigned) * 3 * (size_t)chain_n_);
@@ -447,7 +462,7 @@ class FieldT final : public Field {
     C* vh() { return vh_.as<C>(); }
 
     typename Ops<R>::XP xp() { return xp0<R>(g_, tw_); }
-    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(err_, g_, a, tw_, X); }
+    typename Ops<R>::SP sp(C* a, int X) { return sp0<R>(err_, g_, a, tw_, X, tune_); }
 
     // ---- pass sequences ----
     void y_fwd(C* a, int X) {
@@ -476,7 +491,9 @@ class FieldT final : public Field {
     }
     // psi^_x -> y forward, z drift, y inverse: one slab-ordered kernel (FP32
     // 3D, tune_.chain) or three passes
-    bool chain_on() const { return chain_n_ && tune_.tma && Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, tune_.chain); }
+    bool chain_on() const {
+        return chain_n_ && tune_.tma && tune_.plan == 0 && Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, tune_.chain);
+    }
     void yz_drift(double dt) {
         if (chain_on()) {
             auto s = sp(psi(), g_.N);
@@ -1208,23 +1225,28 @@ class FieldT final : public Field {
             if (from_cache) *from_cache = true;
             return cached_ms;
         }
-        // candidates: pencils per thread, ring depth, y / last-axis tile widths, rows per x block
+        // candidates: radix plan of the strided passes, pencils per thread, ring
+        // depth, y / last-axis tile widths, rows per x block (plan 1 runs 8-column tiles)
         std::vector<Tune> cands;
         const int pws[2] = {sizeof(R) == 4 ? 2 : 1, 1};
-        for (int ip = 0; ip < (sizeof(R) == 4 ? 2 : 1); ++ip)
-            for (int nb : {0, 2, 4})
-                for (int ytx : {8, 16})
-                    for (int latx : {8, 16})
-                        for (int xr : {0, 4}) {
-                            Tune t;
-                            t.pw = pws[ip];
-                            t.nbuf = nb;
-                            t.y_tx = ytx;
-                            t.la_tx = latx;
-                            t.x_rows = xr;
-                            t.tma = 1;
-                            cands.push_back(t);
-                        }
+        const int nplans = Ops<R>::has_plan1(g_.N) ? 2 : 1;
+        for (int plan = 0; plan < nplans; ++plan)
+            for (int ip = 0; ip < (sizeof(R) == 4 ? 2 : 1); ++ip)
+                for (int nb : {0, 2, 4})
+                    for (int ytx : {8, 16})
+                        for (int latx : {8, 16})
+                            for (int xr : {0, 4}) {
+                                if (plan == 1 && (ytx != 8 || latx != 8)) continue;
+                                Tune t;
+                                t.plan = plan;
+                                t.pw = pws[ip];
+                                t.nbuf = nb;
+                                t.y_tx = ytx;
+                                t.la_tx = latx;
+                                t.x_rows = xr;
+                                t.tma = 1;
+                                cands.push_back(t);
+                            }
         // keep the state: tuning advances it
         DevBuf save;
         save.alloc(sizeof(C) * g_.S);
@@ -1264,9 +1286,21 @@ class FieldT final : public Field {
     }
 
     std::string tune_key() const {
-        return std::to_string(g_.dim) + " " + std::to_string(g_.N) + " " + (sizeof(R) == 4 ? "c64" : "c128") + " " +
-               std::to_string(g_.B);
+        return "v2 " + std::to_string(g_.dim) + " " + std::to_string(g_.N) + " " + (sizeof(R) == 4 ? "c64" : "c128") +
+               " " + std::to_string(g_.B);
     }
+
+    // apply a tuned geometry for this grid if the process cache or the file
+    // named by QX_TUNE_CACHE holds one (called at construction)
+    void consult_tune_cache() {
+        Tune t;
+        double ms = 0.0;
+        if (tune_lookup(tune_key(), std::getenv("QX_TUNE_CACHE"), t, ms)) {
+            tune_ = t;
+            tuned_from_cache_ = true;
+        }
+    }
+    bool tuned_from_cache() const override { return tuned_from_cache_; }
 
     // per-pass device time of the loop body, averaged over nsteps bodies
     void profile_step(int nsteps, std::vector<std::pair<std::string, double>>& out) override {
@@ -1362,9 +1396,10 @@ class FieldT final : public Field {
 
   private:
     int device_ = 0;
-    DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, twNn_, red_, redout_, errbuf_;
+    DevBuf psi_, V_, vh_, twN_, twM_, twNl_, twMl_, twNn_, twP_, twPl_, red_, redout_, errbuf_;
     TwTables<C> tw_{};
     int* err_ = nullptr;
+    bool tuned_from_cache_ = false;
     DevBuf axy_;       // drift factor tables A(nx, ny), B(nz)/S (ensure_axy)
     double axy_fac_ = std::numeric_limits<double>::quiet_NaN();
     DevBuf chain_;     // drift chain: [3n] phase counters

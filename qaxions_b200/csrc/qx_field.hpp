@@ -78,6 +78,10 @@ template <typename C> struct TwTables {
     const C* N_lo;
     const C* M_lo;
     const C* N_nat;
+    // N-point stage-major tables of radix plan 1 (qx_with_plan) for the TMA
+    // strided passes, where the grid has that plan (else null)
+    const C* N_p1;
+    const C* N_p1_lo;
 };
 
 template <typename R>
@@ -240,6 +244,8 @@ class Field {
         s_ = time;
     }
     Tune& tune() { return tune_; }
+    // whether construction applied a geometry from the autotuner's cache
+    virtual bool tuned_from_cache() const = 0;
     // drop the captured loop-body graph (after launch geometry changes)
     virtual void invalidate_graph() = 0;
 
@@ -255,6 +261,9 @@ class Field {
 };
 
 std::unique_ptr<Field> make_field(const FieldConfig& cfg);
+
+// forget the autotuner's in-process choices (files are left alone)
+void clear_tune_cache();
 
 // host-side conversion between FFTW's r2c layout and the packed layout
 void pack_half(int dim, int N, const double* fftw_half, double* packed);

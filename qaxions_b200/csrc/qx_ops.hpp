@@ -10,6 +10,10 @@ namespace qx {
 // supported grid sizes N (per axis)
 bool supported_n(int N);
 
+// transform length n tagged with a radix plan (the encoding of qx_with_plan in
+// qx_fft.cuh: the plan index in the bits above 16)
+constexpr int plan_tagged(int n, int plan) { return n | (plan << 16); }
+
 enum XC2R { C2R_WRITE_V = 1, C2R_KICK = 2, C2R_WRITE_PSI = 4, C2R_FWD = 8 };
 enum LaOp { OP_FWD = 0, OP_INV = 1, OP_DRIFT = 2, OP_POISSON = 3, OP_KIN = 4 };
 
@@ -21,6 +25,8 @@ struct Tune {
     int tma = 1;      // strided passes: 1 = persistent TMA-fed kernels, 0 = direct-load kernels
     int nbuf = 0;     // TMA ring depth (0 = as many 64 KB-class tiles as fit in ~200 KB)
     int pw = 0;       // pencils per thread of TMA passes (0 = default: 2 in FP32, 1 in FP64)
+    int plan = 0;     // radix plan of the TMA strided passes: 0 default order, 1 reversed
+                      // (grids whose plan has radices of different sizes: 64, 96, 128, 256)
     int chain = 0;    // FP32 3D drift's y / z / y passes: 0 three passes; 1 / 2 one slab-ordered
                       // kernel over slabs of `chain` 8-column tiles (bit-identical, measured slower)
 };
@@ -42,6 +48,7 @@ template <typename R> struct Ops {
         // drift: the factor tables A(nx, ny), B(nz) of drift_tables (qx_misc.hpp);
         // the TMA drift pass reads them
         const double2* axy;
+        int plan;  // radix plan of the TMA passes; tw / tw_lo are that plan's tables
     };
     static void x_fwd(int N, const XP& a, bool kick, const Tune& tu, cudaStream_t st);
     static void x_inv(int N, const XP& a, bool r2c, const Tune& tu, cudaStream_t st);
@@ -59,9 +66,12 @@ template <typename R> struct Ops {
     // counters, zeroed here) on stream st.
     static int chain_slabs(int N, int dim, int batch, int sw);
     static void drift_chain(int N, const SP& a, int sw, unsigned* cnt, const Tune& tu, cudaStream_t st);
-    // stage-major FFT twiddle table of length L from the natural-order table
-    // nat[j] = exp(-2 pi i j/L) (entries beyond L - r0 are left as they are)
+    // stage-major FFT twiddle table of a (plan-tagged, qx_with_plan) length L
+    // from the natural-order table nat[j] = exp(-2 pi i j/n), n = qx_len(L)
+    // (entries beyond n - r0 are left as they are)
     static void stage_twiddles(const C* nat, int L, C* out);
+    // whether the strided passes of grid size N offer radix plan 1
+    static bool has_plan1(int N);
 };
 
 }  // namespace qx

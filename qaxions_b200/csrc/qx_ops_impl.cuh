@@ -61,13 +61,14 @@ template <typename R> static SArgs<R> to_s(const typename Ops<R>::SP& a) {
 
 template <typename R>
 void Ops<R>::stage_twiddles(const C* nat, int L, C* out) {
-    const int S = qx_nstages(L);
+    const int S = qx_nstages(L), n = qx_len(L);
     for (int s = 1; s < S; ++s) {
-        const int r = qx_radix(L, s), Ns = qx_span(L, s), stw = L / (Ns * r);
+        const int r = qx_radix(L, s), Ns = qx_span(L, s), stw = n / (Ns * r);
         for (int m = 1; m < r; ++m)
-            for (int k = 0; k < Ns; ++k) out[qx_tw_index(L, Ns, m, k)] = nat[(k * m * stw) % L];
+            for (int k = 0; k < Ns; ++k) out[qx_tw_index(L, Ns, m, k)] = nat[(k * m * stw) % n];
     }
 }
+
 
 // rows per block for x passes: T*P ~ 256 threads, P | rows
 static int x_rows_per_block(int N, long rows, int want) {
@@ -281,8 +282,21 @@ template <typename R, int OP> static bool use_df(const typename Ops<R>::SP& a) {
     }
 }
 
-// Run one TMA pencil pass over `a` ([NZ][N][X]).  Returns the grid size.
-template <int NN, typename R, int OP, int PW, bool DF, int TXF>
+static_assert(plan_tagged(96, 1) == qx_with_plan(96, 1), "one plan encoding for host and device");
+
+// grids whose strided passes are also compiled with radix plan 1 (reversed
+// order; only where it differs from the default)
+template <int NN> constexpr bool strided_plan1() { return NN >= 64 && qx_plan1_differs(NN); }
+
+template <typename R>
+bool Ops<R>::has_plan1(int N) {
+    QX_FOR_N(N, { return strided_plan1<NN>(); });
+    return false;
+}
+
+// Run one TMA pencil pass over `a` ([NZ][N][X]) with radix plan PLAN (the SP's
+// twiddle tables are that plan's).  Returns the grid size.
+template <int NN, typename R, int OP, int PW, bool DF, int TXF, int PLAN = 0>
 static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                          const Tune& tu, cudaStream_t st) {
     const TmaGeom g = tma_geom<NN, R, PW, TXF>(a.X, pencil_dim == 2 || outer == 1 ? tu.la_tx : tu.y_tx, OP, tu);
@@ -311,7 +325,7 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     s.err = a.err;
     constexpr bool SWZ = tma_swizzled<NN, R, PW, TXF>();
     const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, g.TX, g.box, pencil_dim, SWZ);
-    auto kern = k_pencil_tma<NN, R, OP, PW, DF, TXF>;
+    auto kern = k_pencil_tma<NN, R, OP, PW, DF, TXF, PLAN>;
     const size_t smem = tma_smem_bytes<R>(NN, g.TX, g.nbuf, OP, SWZ);
     set_smem(kern, smem);
     static int bps_cache[64] = {0};
@@ -341,6 +355,10 @@ static long launch_tma_tx(const typename Ops<R>::SP& a, int NZ, int outer, int p
     } else {
         const int want = (pencil_dim == 2 || outer == 1) ? tu.la_tx : tu.y_tx;
         const int tx = want == 8 || want == 16 ? want : 8;
+        if constexpr (strided_plan1<NN>()) {
+            if (a.plan == 1) return launch_tma_e<NN, R, OP, PW, DF, 8, 1>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
+        }
+        if (a.plan != 0) throw std::logic_error("radix plan not compiled for this grid");
         if constexpr (sizeof(R) == 4 && NN >= 64) {
             if (tx == 16) return launch_tma_e<NN, R, OP, PW, DF, 16>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
         }
@@ -444,6 +462,13 @@ static void launch_col0(const typename Ops<R>::SP& a, cudaStream_t st) {
     constexpr int E0 = qx_lcm_radices(NN);
     dim3 blk(2, NN / E0, 1);
     dim3 grd(NN / 2, a.batch > 0 ? a.batch : 1);
+    if constexpr (strided_plan1<NN>()) {
+        if (a.plan == 1) {
+            k_poisson_col0<NN, R, 1><<<grd, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.tw_lo, a.pois_c, a.pois_g0);
+            QX_LAUNCH_CHECK();
+            return;
+        }
+    }
     k_poisson_col0<NN, R><<<grd, blk, 2 * NN * sizeof(C), st>>>(a.a, a.tw, a.tw_lo, a.pois_c, a.pois_g0);
     QX_LAUNCH_CHECK();
 }

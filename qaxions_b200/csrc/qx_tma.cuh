@@ -191,13 +191,17 @@ template <typename P, bool SWZ> struct TileAcc {
 // blockDim = (TX / PW, N / E, 1), or (TX / PW / 2, N / E, 2) when swizzled:
 // thread (c, t) owns columns x0 + PW c + h (h < PW), c = x + blockDim.x z;
 // TX = TXF when TXF > 0
-template <int N, typename R, int OP, int PW, bool DF, int TXF>
+// PLAN: radix plan of the pencil transforms (qx_with_plan); the twiddle tables
+// passed in TArgs are the stage-major tables of that plan.
+template <int N, typename R, int OP, int PW, bool DF, int TXF, int PLAN = 0>
 __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_block_min<N, R, PW, TXF>()))
     k_pencil_tma(const __grid_constant__ CUtensorMap tm, TArgs<R> s) {
     using C = cx_t<R>;
     using P = pencil_val_t<PW, C>;
     static_assert(PW == 1 || sizeof(R) == 4, "paired pencils are an FP32 layout");
+    constexpr int NL = qx_with_plan(N, PLAN);
     constexpr int E = tma_e<N, R, PW>();
+    static_assert(qx_lcm_radices(NL) == qx_lcm_radices(N), "a plan keeps the elements per thread");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[8];
     __shared__ int s_abort;
@@ -292,12 +296,12 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
         P v[E];
         if constexpr (OP == OP_INV) {
 #pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = acc(out_pos<N, E>(e, t));
-            ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
+            for (int e = 0; e < E; ++e) v[e] = acc(out_pos<NL, E>(e, t));
+            ifft_pencil_rev<NL, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
         } else {
 #pragma unroll
-            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<N, E, 0>(e, t));
-            fft_pencil<N, E, -1>(v, acc, t, tw_src<DF>(tws, tws_lo));
+            for (int e = 0; e < E; ++e) v[e] = acc(in_pos<NL, E, 0>(e, t));
+            fft_pencil<NL, E, -1>(v, acc, t, tw_src<DF>(tws, tws_lo));
         }
 
         // |n|^2 contribution of x (and y in 3D) of pencil h
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
                 const long mxy = mxy_of(h);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    const int nz = signed_mode(out_pos<N, E>(e, t), N);
+                    const int nz = signed_mode(out_pos<NL, E>(e, t), N);
                     const C u = pen(v[e], h);
                     kin += (double)(mxy + (long)nz * nz) * ((double)u.x * (double)u.x + (double)u.y * (double)u.y);
                 }
@@ -328,13 +332,13 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
                 // A(nx, ny) of the thread's columns from the tile's ring slot
                 // (staged before the previous tile's store barrier; a multi-stage
                 // forward transform has synchronised the block since)
-                if constexpr (qx_nstages(N) == 1) __syncthreads();
+                if constexpr (qx_nstages(NL) == 1) __syncthreads();
 #pragma unroll
                 for (int h = 0; h < PW; ++h) {
                     const double2 A = aslot[b * kTmaMaxTX + PW * c + h];
 #pragma unroll
                     for (int e = 0; e < E; ++e)
-                        pen(v[e], h) = cmul_d(pen(v[e], h), dcmul(A, bz[out_pos<N, E>(e, t)]));
+                        pen(v[e], h) = cmul_d(pen(v[e], h), dcmul(A, bz[out_pos<NL, E>(e, t)]));
                 }
             } else {
                 SArgs<R> sa;
@@ -344,17 +348,17 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
                     // 3D: column 0 (kx = 0 and N/2 packed) is paired with its mirror
                     // row by k_poisson_col0; keep the forward result for it
 #pragma unroll
-                    for (int e = 0; e < E; ++e) col0[out_pos<N, E>(e, t)] = pen(v[e], 0);
+                    for (int e = 0; e < E; ++e) col0[out_pos<NL, E>(e, t)] = pen(v[e], 0);
                 } else if (x0 == 0 && !s.col0_external) {
                     // 2D: the mirror -k_y of column 0 lies in the same pencil
                     __syncthreads();
 #pragma unroll
-                    for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+                    for (int e = 0; e < E; ++e) acc(out_pos<NL, E>(e, t)) = v[e];
                     __syncthreads();
                     if (c == 0) {
 #pragma unroll
                         for (int e = 0; e < E; ++e) {
-                            const int p = out_pos<N, E>(e, t);
+                            const int p = out_pos<NL, E>(e, t);
                             const long np = signed_mode(p, N);
                             const long mA = np * np, mB = mA + (long)(N / 2) * (N / 2);
                             const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
@@ -369,21 +373,21 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
                     const long mxy = mxy_of(h);
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
-                        const int nz = signed_mode(out_pos<N, E>(e, t), N);
+                        const int nz = signed_mode(out_pos<NL, E>(e, t), N);
                         pen(v[e], h) = cscale(pen(v[e], h), pois_mult<R>(mxy + (long)nz * nz, sa));
                     }
                 }
             }
             // inverse transform: the forward stages undone in reverse order,
             // from the forward output order back to the load order
-            ifft_pencil_rev<N, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
+            ifft_pencil_rev<NL, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
             if (OP == OP_POISSON && s.col0_external && x0 == 0) {
                 // the stash was written in another order by other threads; a
                 // multi-stage inverse already synchronised the block
-                if constexpr (qx_nstages(N) == 1) __syncthreads();
+                if constexpr (qx_nstages(NL) == 1) __syncthreads();
                 if (c0ext) {
 #pragma unroll
-                    for (int e = 0; e < E; ++e) pen(v[e], 0) = col0[in_pos<N, E, 0>(e, t)];
+                    for (int e = 0; e < E; ++e) pen(v[e], 0) = col0[in_pos<NL, E, 0>(e, t)];
                 }
             }
         }
@@ -394,10 +398,10 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
             __syncthreads();
             if constexpr (OP == OP_FWD) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) acc(out_pos<N, E>(e, t)) = v[e];
+                for (int e = 0; e < E; ++e) acc(out_pos<NL, E>(e, t)) = v[e];
             } else {
 #pragma unroll
-                for (int e = 0; e < E; ++e) acc(in_pos<N, E, 0>(e, t)) = v[e];
+                for (int e = 0; e < E; ++e) acc(in_pos<NL, E, 0>(e, t)) = v[e];
             }
             fence_proxy_async();
             __syncthreads();
@@ -451,10 +455,11 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
 // C'(k) = a C(k) + b conj C(-k) with a, b from the kx = 0 and kx = N/2
 // multipliers, then the inverse z transform.  blockDim = (2, N/E); grid
 // (N/2, boxes of a batched array).
-template <int N, typename R>
+template <int N, typename R, int PLAN = 0>
 __global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, const cx_t<R>* tw_lo, double pois_c,
                                double pois_g0) {
     using C = cx_t<R>;
+    constexpr int NL = qx_with_plan(N, PLAN);
     constexpr int E = qx_lcm_radices(N);
     constexpr int X = N / 2;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -478,16 +483,16 @@ __global__ void k_poisson_col0(cx_t<R>* vh, const cx_t<R>* tw, const cx_t<R>* tw
     C v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-        const int p = out_pos<N, E>(e, t);
+        const int p = out_pos<NL, E>(e, t);
         const long nz = signed_mode(p, N);
         const long mA = ny * ny + nz * nz, mB = mA + (long)X * X;
         const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
         const C cm = cconj(macc((N - p) % N));
         v[e] = cadd(cscale(acc(p), R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
     }
-    ifft_pencil_rev<N, E>(v, acc, t, tw_src<false>(tw, tw_lo));
+    ifft_pencil_rev<NL, E>(v, acc, t, tw_src<false>(tw, tw_lo));
 #pragma unroll
-    for (int e = 0; e < E; ++e) vh[base + (long)in_pos<N, E, 0>(e, t) * pstride] = v[e];
+    for (int e = 0; e < E; ++e) vh[base + (long)in_pos<NL, E, 0>(e, t) * pstride] = v[e];
 }
 
 }  // namespace qx
