@@ -448,6 +448,19 @@ struct qx_ens_s {
     std::vector<int> index_in;  // box -> index within its group
     long long sites = 0;
     std::string err;
+    // one loop body of every group as ONE graph (a branch per group on the
+    // group's stream, forked from and joined into `s0`), replayed once per step
+    cudaStream_t s0 = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<double> exec_dt;  // each group's ds when captured
+    std::vector<cudaEvent_t> ev;  // per group: fork/join events
+    cudaEvent_t ev0 = nullptr;
+    ~qx_ens_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto e : ev) cudaEventDestroy(e);
+        if (ev0) cudaEventDestroy(ev0);
+        if (s0) cudaStreamDestroy(s0);
+    }
 };
 
 namespace {
@@ -603,10 +616,77 @@ int qx_ens_get_psi(qx_ens_t* h, int box, double* psi) {
     });
 }
 
+namespace {
+// s0 waits for every group stream's work so far
+void ens_join(qx_ens_s& e) {
+    for (size_t i = 0; i < e.groups.size(); ++i) {
+        QX_CU(cudaEventRecord(e.ev[i], e.groups[i]->stream()));
+        QX_CU(cudaStreamWaitEvent(e.s0, e.ev[i], 0));
+    }
+}
+// every group stream waits for s0's work so far
+void ens_fork(qx_ens_s& e) {
+    QX_CU(cudaEventRecord(e.ev0, e.s0));
+    for (auto& g : e.groups) QX_CU(cudaStreamWaitEvent(g->stream(), e.ev0, 0));
+}
+
+void ens_capture(qx_ens_s& e) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    e.exec = nullptr;
+    for (auto& g : e.groups) g->prepare_replay();
+    for (auto& g : e.groups) g->sync();
+    cudaGraph_t graph = nullptr;
+    QX_CU(cudaStreamBeginCapture(e.s0, cudaStreamCaptureModeThreadLocal));
+    try {
+        ens_fork(e);  // the group streams join the capture
+        for (auto& g : e.groups) g->enqueue_body(false);
+        ens_join(e);
+    } catch (...) {
+        cudaStreamEndCapture(e.s0, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    QX_CU(cudaStreamEndCapture(e.s0, &graph));
+    const cudaError_t r = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    QX_CU(r);
+    e.exec_dt.clear();
+    for (auto& g : e.groups) e.exec_dt.push_back(g->dt());
+}
+
+// the merged loop of every box: prologues and the first and last bodies run
+// eagerly on the group streams; the bodies in between are one graph replay
+// per step over all groups
+void ens_step(qx_ens_s& e, int nsteps) {
+    if (nsteps <= 0) return;
+    if (!e.s0) {
+        QX_CU(cudaStreamCreateWithFlags(&e.s0, cudaStreamNonBlocking));
+        QX_CU(cudaEventCreateWithFlags(&e.ev0, cudaEventDisableTiming));
+        e.ev.resize(e.groups.size());
+        for (auto& v : e.ev) QX_CU(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
+    }
+    for (auto& g : e.groups) g->step_begin();
+    if (nsteps > 1) {
+        for (auto& g : e.groups) g->enqueue_body(false);  // eager (also sets kernel attributes)
+        if (nsteps > 2) {
+            bool same = e.exec && e.exec_dt.size() == e.groups.size();
+            for (size_t i = 0; same && i < e.groups.size(); ++i) same = e.exec_dt[i] == e.groups[i]->dt();
+            if (!same) ens_capture(e);
+            for (auto& g : e.groups) g->prepare_replay();
+            ens_join(e);
+            for (int i = 0; i < nsteps - 2; ++i) QX_CU(cudaGraphLaunch(e.exec, e.s0));
+            ens_fork(e);
+        }
+    }
+    for (auto& g : e.groups) g->enqueue_body(true);
+    for (auto& g : e.groups) g->step_end(nsteps);
+}
+}  // namespace
+
 int qx_ens_step(qx_ens_t* h, int nsteps) {
     return ens_guarded(h, [&](qx_ens_s& e) {
         need(nsteps >= 0, "nsteps must be >= 0");
-        for (auto& g : e.groups) g->step(nsteps);  // enqueued on each group's stream
+        ens_step(e, nsteps);
         for (auto& g : e.groups) g->sync();
     });
 }
@@ -624,10 +704,8 @@ int qx_ens_time_steps(qx_ens_t* h, int nsteps, float* ms) {
         for (auto& ev : ends) QX_CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         QX_CU(cudaEventRecord(start, s0));
         for (auto& g : e.groups) QX_CU(cudaStreamWaitEvent(g->stream(), start, 0));
-        for (size_t i = 0; i < e.groups.size(); ++i) {
-            e.groups[i]->step(nsteps);
-            QX_CU(cudaEventRecord(ends[i], e.groups[i]->stream()));
-        }
+        ens_step(e, nsteps);
+        for (size_t i = 0; i < e.groups.size(); ++i) QX_CU(cudaEventRecord(ends[i], e.groups[i]->stream()));
         for (auto& ev : ends) QX_CU(cudaStreamWaitEvent(s0, ev, 0));
         QX_CU(cudaEventRecord(stop, s0));
         QX_CU(cudaEventSynchronize(stop));

@@ -605,6 +605,18 @@ class FieldT final : public Field {
         vmax_stale_ = true;
     }
 
+    void step_begin() override {
+        if (cosmo_ != 0) throw std::logic_error("stepping in pieces needs the STATIC cosmology");
+        prologue();
+    }
+    void enqueue_body(bool last) override { body(ds_, ds_, pref_eff(), last); }
+    void step_end(int nsteps) override {
+        for (int i = 0; i < nsteps; ++i) updateTime();
+        v_current_ = true;
+        vmax_stale_ = true;
+    }
+    void prepare_replay() override { ensure_axy(ds_); }
+
     // Poisson source prefactor: pref (STATIC) or norm a with norm = 1 (MRE,
     // src/field.cxx:84-86,298)
     double pref_eff() const { return cosmo_ == 1 ? a_ : cfg_.pref; }

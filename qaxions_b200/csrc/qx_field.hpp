@@ -157,6 +157,15 @@ class Field {
     // merged leapfrog of src/main.cxx:64-85 (measurements off), fused passes,
     // loop body replayed from a CUDA graph
     virtual void step(int nsteps) = 0;
+    // step() in pieces, for a caller that replays several fields' loop bodies
+    // in one CUDA graph of its own (an ensemble; STATIC cosmology): the
+    // prologue, one loop body on the field's stream (last: the final body,
+    // ending in the half kick), the clock advance of nsteps, and what a
+    // replay of a captured body needs first (the drift factor tables of ds)
+    virtual void step_begin() = 0;
+    virtual void enqueue_body(bool last) = 0;
+    virtual void step_end(int nsteps) = 0;
+    virtual void prepare_replay() = 0;
     // measure() (src/meas.cxx:13-63) without overwriting V (unless the mask
     // has MEAS_CLOBBER_V); files go to `dir` when it is not null
     virtual void measure(unsigned mask, int number, const char* dir, MeasRecord* rec) = 0;

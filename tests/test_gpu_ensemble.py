@@ -46,3 +46,28 @@ def test_ensemble_timing_and_errors():
     with pytest.raises(ValueError):
         qx.Ensemble([(33, 1)])
     ens.close()
+
+
+@pytest.mark.parametrize("dtype", ["c128", "c64"])
+def test_ensemble_graph_replays_across_calls(dtype):
+    """The loop bodies of all groups replay as one graph per step; calls of
+    different lengths in a row (graph reused, and the 1- and 2-step calls that
+    need no graph) leave every box as its single-box run with the same calls."""
+    groups = [(32, 2), (96, 1), (64, 1)]
+    dt = 0.2 / 96**2
+    calls = (5, 1, 2, 7)
+    ens = qx.Ensemble(groups, dtype=dtype, dt=dt)
+    ens.ic_config(qx.IC_GRF, seed_base=40, n_sol=1)
+    for n in calls:
+        ens.step(n)
+    b = 0
+    for n, c in groups:
+        for _ in range(c):
+            f = qx.Field(3, n, dtype=dtype, k0="zero", dt=dt)
+            f.ic_config(qx.IC_GRF, 40 + b, 1, 0.01, 0.03)
+            for k in calls:
+                f.step(k)
+            assert O.rel_l2(ens.psi(b), f.psi) <= TOL[dtype], (n, b)
+            f.close()
+            b += 1
+    ens.close()
