@@ -182,10 +182,18 @@ int qx_set_tune(qx_field_t *h, int x_rows, int y_tx, int la_tx, int tma, int nbu
  * order, for grids whose default plan mixes radix sizes (N = 64, 96, 128,
  * 256); elsewhere plan 1 runs as plan 0.  Results agree to round-off. */
 int qx_set_plan(qx_field_t *h, int plan);
-/* the launch geometry in use: out[9] = {x_rows, y_tx, la_tx, tma, nbuf, pw,
- * plan, chain, from_cache}; from_cache = 1 when the field took it from the
- * autotuner's cache at creation (the process cache, or the file named by the
- * environment variable QX_TUNE_CACHE) */
+/* Pencil-to-thread mapping of the FP32 strided passes at N = 256 and 512 (no
+ * counterpart in the reference): 8-column tiles with a pencil pair per 64
+ * (N = 512) threads and block-wide stage exchanges, or 16-column swizzled tiles
+ * with one warp per pencil pair, warp-local exchanges and one block barrier
+ * per tile.  on = 0: the 8-column passes everywhere; 1: the warp passes for
+ * the wave-function arrays (the 3D 512^3 default, measured fastest); 2: the
+ * warp passes everywhere.  Results agree to round-off. */
+int qx_set_pencil_warp(qx_field_t *h, int on);
+/* the launch geometry in use: out[10] = {x_rows, y_tx, la_tx, tma, nbuf, pw,
+ * plan, chain, pencil_warp, from_cache}; from_cache = 1 when the field took it
+ * from the autotuner's cache at creation (the process cache, or the file named
+ * by the environment variable QX_TUNE_CACHE) */
 int qx_get_tune(qx_field_t *h, int *out, int n);
 /* Drift chain (no counterpart in the reference: the reference's drift,
  * src/field.cxx:119-198, is three library FFT calls around a multiply).  on = 0

@@ -95,6 +95,7 @@ _SIGS = {
     "qx_set_tune": ([_vp, _i, _i, _i, _i, _i, _i], _i),
     "qx_set_chain": ([_vp, _i], _i),
     "qx_set_plan": ([_vp, _i], _i),
+    "qx_set_pencil_warp": ([_vp, _i], _i),
     "qx_clear_tune_cache": ([], _i),
     "qx_get_tune": ([_vp, _ip, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
@@ -432,10 +433,16 @@ class Field:
     def get_tune(self) -> dict:
         """The launch geometry in use (and whether it came from the autotuner's
         cache when the field was created)."""
-        v = (C.c_int * 9)()
-        self._c("qx_get_tune", v, 9)
-        keys = ("x_rows", "y_tx", "la_tx", "tma", "nbuf", "pw", "plan", "chain", "from_cache")
+        v = (C.c_int * 10)()
+        self._c("qx_get_tune", v, 10)
+        keys = ("x_rows", "y_tx", "la_tx", "tma", "nbuf", "pw", "plan", "chain", "pencil_warp", "from_cache")
         return dict(zip(keys, list(v)))
+
+    def set_pencil_warp(self, on):
+        """FP32 strided passes at N = 256, 512: one warp per pencil pair in
+        16-column swizzled tiles for the wave-function passes (1 / True), for
+        every strided pass (2), or 8-column tiles everywhere (0 / False)."""
+        self._c("qx_set_pencil_warp", int(on))
 
     def set_chain(self, on):
         """Drift chain: the y, z-drift, y passes of a 3D complex64 field as

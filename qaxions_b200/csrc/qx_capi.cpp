@@ -292,12 +292,21 @@ int qx_set_plan(qx_field_t* h, int plan) {
     });
 }
 
+int qx_set_pencil_warp(qx_field_t* h, int on) {
+    return guarded(h, [&](qx::Field& f) {
+        need(on >= 0 && on <= 2, "on must be 0, 1 or 2");
+        f.tune().wp = on;
+        f.invalidate_graph();
+    });
+}
+
 int qx_get_tune(qx_field_t* h, int* out, int n) {
     return guarded(h, [&](qx::Field& f) {
-        need(out && n >= 9, "out must hold 9 ints");
+        need(out && n >= 10, "out must hold 10 ints");
         const qx::Tune& t = f.tune();
-        const int v[9] = {t.x_rows, t.y_tx, t.la_tx, t.tma, t.nbuf, t.pw, t.plan, t.chain, f.tuned_from_cache() ? 1 : 0};
-        for (int i = 0; i < 9; ++i) out[i] = v[i];
+        const int v[10] = {t.x_rows, t.y_tx, t.la_tx, t.tma, t.nbuf, t.pw, t.plan, t.chain, t.wp,
+                           f.tuned_from_cache() ? 1 : 0};
+        for (int i = 0; i < 10; ++i) out[i] = v[i];
     });
 }
 

@@ -334,7 +334,7 @@ void Field::propagate() {  // src/field.cxx:388-402
 }
 
 // ---------------------------------------------------------------------------
-// autotuner cache: "v2 dim N dtype batch : x_rows y_tx la_tx tma nbuf pw plan ms"
+// autotuner cache: "v3 dim N dtype batch : x_rows y_tx la_tx tma nbuf pw plan wp ms"
 // ---------------------------------------------------------------------------
 
 static std::map<std::string, std::pair<Tune, double>>& tune_cache() {
@@ -356,7 +356,7 @@ static bool tune_lookup(const std::string& key, const char* path, Tune& t, doubl
             std::istringstream vs(line.substr(colon + 3));
             Tune u;
             double m = 0.0;
-            if (vs >> u.x_rows >> u.y_tx >> u.la_tx >> u.tma >> u.nbuf >> u.pw >> u.plan >> m) c[key] = {u, m};
+            if (vs >> u.x_rows >> u.y_tx >> u.la_tx >> u.tma >> u.nbuf >> u.pw >> u.plan >> u.wp >> m) c[key] = {u, m};
         }
         it = c.find(key);
     }
@@ -371,7 +371,7 @@ static void tune_store(const std::string& key, const char* path, const Tune& t, 
     if (path && *path) {
         std::ofstream out(path, std::ios::app);
         out << key << " : " << t.x_rows << " " << t.y_tx << " " << t.la_tx << " " << t.tma << " " << t.nbuf << " "
-            << t.pw << " " << t.plan << " " << ms << "\n";
+            << t.pw << " " << t.plan << " " << t.wp << " " << ms << "\n";
     }
 }
 
@@ -437,6 +437,9 @@ class FieldT final : public Field {
         QX_CUDA(cudaMemsetAsync(V_.p, 0, V_.bytes, st_));
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
         fft_ = std::make_unique<B200FFTBackend<R>>(g_, tw_, &tune_, st_, err_);
+        // measured default: at 512^3 FP32 the wave-function passes run faster with
+        // one warp per pencil pair, the half-spectrum passes with the 8-column tiles
+        if (sizeof(R) == 4 && cfg.dim == 3 && cfg.N == 512) tune_.wp = 1;
         consult_tune_cache();
         // drift chain: phase counters (as many as 8-column slabs need)
         chain_n_ = Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, 1);
@@ -1259,6 +1262,20 @@ class FieldT final : public Field {
                                 t.tma = 1;
                                 cands.push_back(t);
                             }
+        // one warp per pencil pair (FP32 N = 256, 512) for the wave-function passes
+        // (wp 1, the half-spectrum passes on the default tiles) or all (wp 2)
+        if (sizeof(R) == 4 && (g_.N == 256 || g_.N == 512))
+            for (int wp : {1, 2})
+                for (int nb : {0, 2})
+                    for (int xr : {0, 4}) {
+                        Tune t;
+                        t.wp = wp;
+                        t.pw = 2;
+                        t.nbuf = nb;
+                        t.x_rows = xr;
+                        t.tma = 1;
+                        cands.push_back(t);
+                    }
         // keep the state: tuning advances it
         DevBuf save;
         save.alloc(sizeof(C) * g_.S);
@@ -1298,7 +1315,7 @@ class FieldT final : public Field {
     }
 
     std::string tune_key() const {
-        return "v2 " + std::to_string(g_.dim) + " " + std::to_string(g_.N) + " " + (sizeof(R) == 4 ? "c64" : "c128") +
+        return "v3 " + std::to_string(g_.dim) + " " + std::to_string(g_.N) + " " + (sizeof(R) == 4 ? "c64" : "c128") +
                " " + std::to_string(g_.B);
     }
 

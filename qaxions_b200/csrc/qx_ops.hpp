@@ -25,6 +25,9 @@ struct Tune {
     int tma = 1;      // strided passes: 1 = persistent TMA-fed kernels, 0 = direct-load kernels
     int nbuf = 0;     // TMA ring depth (0 = as many 64 KB-class tiles as fit in ~200 KB)
     int pw = 0;       // pencils per thread of TMA passes (0 = default: 2 in FP32, 1 in FP64)
+    int wp = 0;       // FP32 strided passes at N = 256 / 512 with one warp per pencil pair
+                      // (16-column swizzled tiles, warp-local stage exchanges): 1 for the
+                      // wave-function arrays' passes, 2 for every strided pass, 0 none
     int plan = 0;     // radix plan of the TMA strided passes: 0 default order, 1 reversed
                       // (grids whose plan has radices of different sizes: 64, 96, 128, 256)
     int chain = 0;    // FP32 3D drift's y / z / y passes: 0 three passes; 1 / 2 one slab-ordered

@@ -343,6 +343,52 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
     return grid;
 }
 
+// Warp-per-pencil-pair pass (k_pencil_wp): FP32, N = 256 / 512, paired
+// pencils, 16-column swizzled tiles, a 3-deep ring, one 8-warp block per SM.
+template <int NN, typename R, int OP, bool DF>
+static long launch_wp(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
+                      cudaStream_t st) {
+    if constexpr (sizeof(R) == 4 && wp_supported(NN)) {
+        constexpr int TX = kWpTX;
+        if (a.X % TX) throw std::logic_error("warp-pencil pass: columns not a multiple of 16");
+        TArgs<R> s;
+        s.tw = a.tw;
+        s.tw_lo = a.tw_lo;
+        s.X = a.X;
+        s.N = NN;
+        s.outer = outer;
+        s.pencil_dim = pencil_dim;
+        s.la3d = la3d;
+        s.TX = TX;
+        s.tiles_x = a.X / TX;
+        s.nbuf = 3;
+        s.box = NN <= 256 ? NN : 256;
+        s.nbox = NN / s.box;
+        s.n_tiles = (long)s.tiles_x * outer;
+        s.phase_fac = a.phase_fac;
+        s.scale = a.scale;
+        s.pois_c = a.pois_c;
+        s.pois_g0 = a.pois_g0;
+        s.col0_external = col0_ext;
+        s.axy = a.axy;
+        if (OP == OP_DRIFT && !a.axy) throw std::logic_error("drift pass needs the A(nx, ny) table");
+        s.partial = a.partial;
+        s.err = a.err;
+        const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, TX, s.box, pencil_dim, true);
+        auto kern = k_pencil_wp<NN, OP, DF>;
+        const size_t smem = tma_smem_bytes<R>(NN, TX, s.nbuf, OP, true);
+        set_smem(kern, smem);
+        long grid = (long)sm_count();
+        if (grid > s.n_tiles) grid = s.n_tiles;
+        kern<<<(unsigned)grid, dim3(32, kWpThreads / 32), smem, st>>>(tm, s);
+        QX_LAUNCH_CHECK();
+        return grid;
+    } else {
+        (void)a, (void)NZ, (void)outer, (void)pencil_dim, (void)la3d, (void)col0_ext, (void)st;
+        throw std::logic_error("warp-pencil pass not compiled for this grid / precision");
+    }
+}
+
 // tile columns: tu.la_tx (last axis) / tu.y_tx (y passes) when 8 or 16, else 8
 // (FP32 16 is compiled for N >= 64: it streams z pencils faster, but at 512^3
 // the FP32 passes are compute-bound and one 512-thread block per SM loses
@@ -355,6 +401,11 @@ static long launch_tma_tx(const typename Ops<R>::SP& a, int NZ, int outer, int p
     } else {
         const int want = (pencil_dim == 2 || outer == 1) ? tu.la_tx : tu.y_tx;
         const int tx = want == 8 || want == 16 ? want : 8;
+        if constexpr (sizeof(R) == 4 && PW == 2 && wp_supported(NN)) {
+            // wp 1: the wave-function arrays' passes (X = N), wp 2: every strided pass
+            if (a.plan == 0 && (tu.wp == 2 || (tu.wp == 1 && a.X == NN)))
+                return launch_wp<NN, R, OP, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, st);
+        }
         if constexpr (strided_plan1<NN>()) {
             if (a.plan == 1) return launch_tma_e<NN, R, OP, PW, DF, 8, 1>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);
         }

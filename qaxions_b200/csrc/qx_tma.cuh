@@ -450,6 +450,273 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-pencil-pair strided pass (FP32, N = 256 or 512).
+//
+// Tiles of 16 columns x N positions (128-byte rows, TMA 128-byte swizzle: the
+// 16-byte pencil pair q of row r sits in chunk q ^ (r & 7)) stream through a
+// 3-deep ring; one block of 8 warps per SM; warp w transforms the pencil pair
+// of columns x0 + 2w, x0 + 2w + 1 with E = N/32 values of each pencil per lane.
+// A pencil pair lives in its warp's own 16-byte slots of the tile, so the FFT
+// stage exchanges need only __syncwarp: the block synchronises once per tile,
+// before the tensor store.  The exchanges address element p at row
+// sigma(p) = p ^ ((p >> 3) & 7) of those slots, which keeps every exchange of
+// the 512- and 256-point plans and the tile's own (identity) rows free of
+// bank conflicts (checked on the CPU with a model of the banks); loads from and
+// stores to the tensor copy use the identity rows.
+// ---------------------------------------------------------------------------
+
+// a pencil pair's element p in the tensor copy's row p of a swizzled tile
+template <typename P> struct SwzRowAcc {
+    P* base;
+    int c;
+    __device__ __forceinline__ P& operator()(int p) const { return base[p * 8 + (c ^ (p & 7))]; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+// the same slots with the exchange rows sigma(p)
+template <typename P> struct WarpXAcc {
+    P* base;
+    int c;
+    __device__ __forceinline__ P& operator()(int p) const {
+        const int r = p ^ ((p >> 3) & 7);
+        return base[r * 8 + (c ^ (r & 7))];
+    }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+
+constexpr int kWpTX = 16;        // tile columns
+constexpr int kWpThreads = 256;  // 8 warps, one pencil pair each
+
+__host__ __device__ constexpr bool wp_supported(int N) { return N == 256 || N == 512; }
+
+// blockDim = (32, 8): lane t = threadIdx.x, pencil pair c = threadIdx.y
+template <int N, int OP, bool DF, int PLAN = 0>
+__global__ void __launch_bounds__(kWpThreads, 1) k_pencil_wp(const __grid_constant__ CUtensorMap tm, TArgs<float> s) {
+    using R = float;
+    using C = float2;
+    using P = CPair<C>;
+    static_assert(wp_supported(N), "warp-per-pencil passes are compiled for N = 256, 512");
+    constexpr int NL = qx_with_plan(N, PLAN);
+    constexpr int E = N / 32;
+    static_assert(E % qx_lcm_radices(NL) == 0, "N/32 values per lane must hold whole butterflies");
+    constexpr int TX = kWpTX;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[8];
+    __shared__ int s_abort;
+    __shared__ double red[32];
+    const int t = threadIdx.x, c = threadIdx.y;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    const int nthr = kWpThreads;
+    const uint32_t tile_bytes = (uint32_t)((size_t)N * TX * sizeof(C));
+    const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
+    C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    C* tws = bufs + s.nbuf * tile_elems;
+    C* tws_lo = tws + N;
+    double2* bz = reinterpret_cast<double2*>(tws_lo + N);
+    double2* aslot = bz + N;
+    C* col0 = reinterpret_cast<C*>(bz + (OP == OP_DRIFT ? N + s.nbuf * kTmaMaxTX : 0));
+    auto a_of_tile = [&](long id, int j) {
+        const int ox = (int)(id / s.tiles_x);
+        return s.axy + (s.la3d ? (long)(ox % N) * N : 0L) + (id % s.tiles_x) * TX + j;
+    };
+    auto coords = [&](long id, int j, int& c0, int& c1, int& c2) {
+        const int x0 = (int)(id % s.tiles_x) * TX;
+        const int o = (int)(id / s.tiles_x);
+        c0 = 2 * x0;
+        if (s.pencil_dim == 1) { c1 = j * s.box; c2 = o; }
+        else { c1 = o % N; c2 = (o / N) * N + j * s.box; }
+    };
+    auto issue_load = [&](long id, int b) {
+        const uint32_t bar = smem_u32(&mbar[b]);
+        mbar_expect_tx(bar, tile_bytes);
+        for (int j = 0; j < s.nbox; ++j) {
+            int c0, c1, c2;
+            coords(id, j, c0, c1, c2);
+            tma_load_3d(smem_u32(bufs + b * tile_elems + (long)j * s.box * TX), &tm, c0, c1, c2, bar);
+        }
+    };
+
+    for (int i = tid; i < N; i += nthr) {
+        tws[i] = s.tw[i];
+        if constexpr (DF) tws_lo[i] = s.tw_lo[i];
+    }
+    if constexpr (OP == OP_DRIFT) {
+        const double2* gbz = s.axy + (s.la3d ? (long)N * N : (long)N);
+        for (int i = tid; i < N; i += nthr) bz[i] = gbz[i];
+        if (blockIdx.x < s.n_tiles && tid < TX) aslot[tid] = *a_of_tile(blockIdx.x, tid);
+    }
+    if (tid == 0) {
+        s_abort = 0;
+        for (int b = 0; b < s.nbuf; ++b) mbar_init(smem_u32(&mbar[b]), 1);
+        fence_mbar_init();
+        for (int k = 0; k < s.nbuf - 1; ++k) {
+            const long id = blockIdx.x + (long)k * gridDim.x;
+            if (id < s.n_tiles) issue_load(id, k);
+        }
+    }
+    __syncthreads();
+
+    double kin = 0.0;
+    int k = 0;
+    for (;; ++k) {
+        const long id = blockIdx.x + (long)k * gridDim.x;
+        if (id >= s.n_tiles) break;
+        const int b = k % s.nbuf;
+        const uint32_t parity = (uint32_t)((k / s.nbuf) & 1);
+        if (!mbar_wait_bounded(smem_u32(&mbar[b]), parity)) s_abort = 1;
+        C* tile = bufs + b * tile_elems;
+        const int x0 = (int)(id % s.tiles_x) * TX;
+        const int o = (int)(id / s.tiles_x);
+        const int xb = x0 + 2 * c;
+        SwzRowAcc<P> io{reinterpret_cast<P*>(tile), c};
+        WarpXAcc<P> acc{reinterpret_cast<P*>(tile), c};
+        const long id_next = id + gridDim.x;
+        const bool a_copy = OP == OP_DRIFT && tid < TX && id_next < s.n_tiles;
+        if (a_copy) {
+            cp_async16(&aslot[((k + 1) % s.nbuf) * kTmaMaxTX + tid], a_of_tile(id_next, tid));
+            cp_async_commit();
+        }
+        P v[E];
+        if constexpr (OP == OP_INV) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = io(out_pos<NL, E>(e, t));
+            ifft_pencil_rev<NL, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
+        } else {
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = io(in_pos<NL, E, 0>(e, t));
+            fft_pencil<NL, E, -1>(v, acc, t, tw_src<DF>(tws, tws_lo));
+        }
+        auto mxy_of = [&](int h) {
+            const int x = xb + h;
+            const int nx = (s.X == N) ? signed_mode(x, N) : x;
+            const int ny = s.la3d ? signed_mode(o % N, N) : 0;
+            return (long)nx * nx + (long)ny * ny;
+        };
+        bool store = true;
+        if constexpr (OP == OP_KIN) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const long mxy = mxy_of(h);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int nz = signed_mode(out_pos<NL, E>(e, t), N);
+                    const C u = pen(v[e], h);
+                    kin += (double)(mxy + (long)nz * nz) * ((double)u.x * (double)u.x + (double)u.y * (double)u.y);
+                }
+            }
+            store = false;
+        } else if constexpr (OP == OP_DRIFT || OP == OP_POISSON) {
+            const bool has_col0 = x0 == 0 && c == 0;
+            const bool c0ext = (OP == OP_POISSON) && s.col0_external && has_col0;
+            if constexpr (OP == OP_DRIFT) {
+                // A(nx, ny) from the tile's ring slot, written before the previous
+                // tile's block barrier
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const double2 A = aslot[b * kTmaMaxTX + 2 * c + h];
+#pragma unroll
+                    for (int e = 0; e < E; ++e)
+                        pen(v[e], h) = cmul_d(pen(v[e], h), dcmul(A, bz[out_pos<NL, E>(e, t)]));
+                }
+            } else {
+                SArgs<R> sa;
+                sa.pois_c = s.pois_c;
+                sa.pois_g0 = s.pois_g0;
+                if (c0ext) {
+                    // 3D: column 0 is finished by k_poisson_col0; keep its forward result
+#pragma unroll
+                    for (int e = 0; e < E; ++e) col0[out_pos<NL, E>(e, t)] = pen(v[e], 0);
+                } else if (has_col0 && !s.col0_external) {
+                    // 2D: the mirror -k_y of column 0 lies in the same pencil (this warp's)
+                    __syncwarp();
+#pragma unroll
+                    for (int e = 0; e < E; ++e) acc(out_pos<NL, E>(e, t)) = v[e];
+                    __syncwarp();
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        const int p = out_pos<NL, E>(e, t);
+                        const long np = signed_mode(p, N);
+                        const long mA = np * np, mB = mA + (long)(N / 2) * (N / 2);
+                        const R gA = pois_mult<R>(mA, sa), gB = pois_mult<R>(mB, sa);
+                        const C cm = cconj(pen(acc((N - p) % N), 0));
+                        pen(v[e], 0) = cadd(cscale(pen(v[e], 0), R(0.5) * (gA + gB)), cscale(cm, R(0.5) * (gA - gB)));
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (h == 0 && has_col0) continue;
+                    const long mxy = mxy_of(h);
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        const int nz = signed_mode(out_pos<NL, E>(e, t), N);
+                        pen(v[e], h) = cscale(pen(v[e], h), pois_mult<R>(mxy + (long)nz * nz, sa));
+                    }
+                }
+            }
+            ifft_pencil_rev<NL, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
+            if (c0ext) {
+                // the stash was written by other lanes of this warp in another order;
+                // the inverse's exchanges synchronised the warp since
+#pragma unroll
+                for (int e = 0; e < E; ++e) pen(v[e], 0) = col0[in_pos<NL, E, 0>(e, t)];
+            }
+        }
+
+        if (a_copy) cp_async_wait_all();
+        if (store) {
+            // the warp's finished pencil pair -> its slots (identity rows) -> tensor store
+            __syncwarp();
+            if constexpr (OP == OP_FWD) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) io(out_pos<NL, E>(e, t)) = v[e];
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) io(in_pos<NL, E, 0>(e, t)) = v[e];
+            }
+            fence_proxy_async();
+            __syncthreads();
+            if (s_abort) break;
+            if (tid == 0) {
+                for (int j = 0; j < s.nbox; ++j) {
+                    int c0, c1, c2;
+                    coords(id, j, c0, c1, c2);
+                    tma_store_3d(&tm, c0, c1, c2, smem_u32(tile + (long)j * s.box * TX));
+                }
+                bulk_commit();
+            }
+        } else {
+            __syncthreads();
+            if (s_abort) break;
+        }
+        if (tid == 0) {
+            const long nid = id + (long)(s.nbuf - 1) * gridDim.x;
+            if (nid < s.n_tiles) {
+                bulk_wait_read_1();
+                fence_proxy_async();
+                issue_load(nid, (k + s.nbuf - 1) % s.nbuf);
+            }
+        }
+    }
+    if (s_abort) {
+        if (tid == 0) {
+            atomicExch(s.err, 1);
+            for (int j = 0; j < s.nbuf - 1; ++j) {
+                const long jd = blockIdx.x + (long)(k + j) * gridDim.x;
+                if (jd < s.n_tiles)
+                    mbar_wait_bounded(smem_u32(&mbar[(k + j) % s.nbuf]), (uint32_t)(((k + j) / s.nbuf) & 1),
+                                      1LL << 28);
+            }
+            bulk_wait_all();
+        }
+        return;
+    }
+    if (tid == 0) bulk_wait_all();
+    if constexpr (OP == OP_KIN) {
+        const double tot = block_reduce<0>(kin, red);
+        if (tid == 0) s.partial[blockIdx.x] = tot;
+    }
+}
+
 // 3D Poisson, column 0: rows y and N-y (0 pairs with N/2) of the packed
 // kx = {0, N/2} column, already transformed along x, y and z, get
 // C'(k) = a C(k) + b conj C(-k) with a, b from the kx = 0 and kx = N/2

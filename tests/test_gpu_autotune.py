@@ -39,14 +39,15 @@ def test_autotune_keeps_state_and_caches(tmp_path, dtype):
     # the tuned geometry steps like the default one
     g.set_tune()
     g.set_plan(0)
+    g.set_pencil_warp(False)
     g.ic_config(qx.IC_GRF, 3, 2, 0.01, 0.03)
     f.step(5)
     g.step(5)
     tol = 1e-12 if dtype == "c128" else 1e-5
     assert np.linalg.norm(f.psi - g.psi) / np.linalg.norm(g.psi) < tol
     lines = open(path).read().splitlines()
-    assert len(lines) == 1 and lines[0].startswith(f"v2 3 64 {dtype} 1 : ")
-    assert len(lines[0].split(" : ")[1].split()) == 8  # x_rows y_tx la_tx tma nbuf pw plan ms
+    assert len(lines) == 1 and lines[0].startswith(f"v3 3 64 {dtype} 1 : ")
+    assert len(lines[0].split(" : ")[1].split()) == 9  # x_rows y_tx la_tx tma nbuf pw plan wp ms
     f.close()
     g.close()
 
