@@ -187,8 +187,11 @@ int qx_set_plan(qx_field_t *h, int plan);
  * (N = 512) threads and block-wide stage exchanges, or 16-column swizzled tiles
  * with one warp per pencil pair, warp-local exchanges and one block barrier
  * per tile.  on = 0: the 8-column passes everywhere; 1: the warp passes for
- * the wave-function arrays (the 3D 512^3 default, measured fastest); 2: the
- * warp passes everywhere.  Results agree to round-off. */
+ * the wave-function arrays; 2: the warp passes everywhere; 3 / 4 (N = 512):
+ * as 1, with each pencil pair split over two warps (16 warps per SM, pair
+ * barriers) in the drift pass / in every wave-function pass, bit for bit the
+ * one-warp form.  The 3D 512^3 default is 3 (measured fastest).  Results
+ * agree to round-off. */
 int qx_set_pencil_warp(qx_field_t *h, int on);
 /* the launch geometry in use: out[10] = {x_rows, y_tx, la_tx, tma, nbuf, pw,
  * plan, chain, pencil_warp, from_cache}; from_cache = 1 when the field took it

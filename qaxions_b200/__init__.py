@@ -441,7 +441,9 @@ class Field:
     def set_pencil_warp(self, on):
         """FP32 strided passes at N = 256, 512: one warp per pencil pair in
         16-column swizzled tiles for the wave-function passes (1 / True), for
-        every strided pass (2), or 8-column tiles everywhere (0 / False)."""
+        every strided pass (2), or 8-column tiles everywhere (0 / False); at
+        N = 512, 3 / 4 split each pencil pair over two warps in the drift pass /
+        in every wave-function pass (bit for bit 1)."""
         self._c("qx_set_pencil_warp", int(on))
 
     def set_chain(self, on):

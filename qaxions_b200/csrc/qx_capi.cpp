@@ -294,7 +294,7 @@ int qx_set_plan(qx_field_t* h, int plan) {
 
 int qx_set_pencil_warp(qx_field_t* h, int on) {
     return guarded(h, [&](qx::Field& f) {
-        need(on >= 0 && on <= 2, "on must be 0, 1 or 2");
+        need(on >= 0 && on <= 4, "on must be 0 ... 4");
         f.tune().wp = on;
         f.invalidate_graph();
     });

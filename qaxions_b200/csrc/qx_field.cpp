@@ -438,8 +438,9 @@ class FieldT final : public Field {
         QX_CUDA(cudaMemsetAsync(vh_.p, 0, vh_.bytes, st_));
         fft_ = std::make_unique<B200FFTBackend<R>>(g_, tw_, &tune_, st_, err_);
         // measured default: at 512^3 FP32 the wave-function passes run faster with
-        // one warp per pencil pair, the half-spectrum passes with the 8-column tiles
-        if (sizeof(R) == 4 && cfg.dim == 3 && cfg.N == 512) tune_.wp = 1;
+        // one warp per pencil pair (the drift pass with two warps per pair), the
+        // half-spectrum passes with the 8-column tiles
+        if (sizeof(R) == 4 && cfg.dim == 3 && cfg.N == 512) tune_.wp = 3;
         consult_tune_cache();
         // drift chain: phase counters (as many as 8-column slabs need)
         chain_n_ = Ops<R>::chain_slabs(g_.N, g_.dim, g_.B, 1);
@@ -1263,9 +1264,12 @@ class FieldT final : public Field {
                                 cands.push_back(t);
                             }
         // one warp per pencil pair (FP32 N = 256, 512) for the wave-function passes
-        // (wp 1, the half-spectrum passes on the default tiles) or all (wp 2)
+        // (wp 1, the half-spectrum passes on the default tiles) or all (wp 2); at
+        // N = 512 also two warps per pair in the drift pass (3) or in every
+        // wave-function pass (4)
         if (sizeof(R) == 4 && (g_.N == 256 || g_.N == 512))
-            for (int wp : {1, 2})
+            for (int wp : {1, 2, 3, 4}) {
+                if (wp > 2 && g_.N != 512) continue;
                 for (int nb : {0, 2})
                     for (int xr : {0, 4}) {
                         Tune t;
@@ -1276,6 +1280,7 @@ class FieldT final : public Field {
                         t.tma = 1;
                         cands.push_back(t);
                     }
+            }
         // keep the state: tuning advances it
         DevBuf save;
         save.alloc(sizeof(C) * g_.S);

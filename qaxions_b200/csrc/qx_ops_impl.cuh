@@ -344,8 +344,9 @@ static long launch_tma_e(const typename Ops<R>::SP& a, int NZ, int outer, int pe
 }
 
 // Warp-per-pencil-pair pass (k_pencil_wp): FP32, N = 256 / 512, paired
-// pencils, 16-column swizzled tiles, a 3-deep ring, one 8-warp block per SM.
-template <int NN, typename R, int OP, bool DF>
+// pencils, 16-column swizzled tiles, a 3-deep ring, one block per SM of 8 warps
+// (WPP = 1) or 16 warps, two per pencil pair (WPP = 2).
+template <int NN, typename R, int OP, bool DF, int WPP = 1>
 static long launch_wp(const typename Ops<R>::SP& a, int NZ, int outer, int pencil_dim, int la3d, int col0_ext,
                       cudaStream_t st) {
     if constexpr (sizeof(R) == 4 && wp_supported(NN)) {
@@ -375,12 +376,12 @@ static long launch_wp(const typename Ops<R>::SP& a, int NZ, int outer, int penci
         s.partial = a.partial;
         s.err = a.err;
         const CUtensorMap tm = make_tmap<R>(a.a, a.X, NN, NZ, TX, s.box, pencil_dim, true);
-        auto kern = k_pencil_wp<NN, OP, DF>;
+        auto kern = k_pencil_wp<NN, OP, DF, 0, WPP>;
         const size_t smem = tma_smem_bytes<R>(NN, TX, s.nbuf, OP, true);
         set_smem(kern, smem);
         long grid = (long)sm_count();
         if (grid > s.n_tiles) grid = s.n_tiles;
-        kern<<<(unsigned)grid, dim3(32, kWpThreads / 32), smem, st>>>(tm, s);
+        kern<<<(unsigned)grid, dim3(32 * WPP, kWpThreads / 32), smem, st>>>(tm, s);
         QX_LAUNCH_CHECK();
         return grid;
     } else {
@@ -402,9 +403,16 @@ static long launch_tma_tx(const typename Ops<R>::SP& a, int NZ, int outer, int p
         const int want = (pencil_dim == 2 || outer == 1) ? tu.la_tx : tu.y_tx;
         const int tx = want == 8 || want == 16 ? want : 8;
         if constexpr (sizeof(R) == 4 && PW == 2 && wp_supported(NN)) {
-            // wp 1: the wave-function arrays' passes (X = N), wp 2: every strided pass
-            if (a.plan == 0 && (tu.wp == 2 || (tu.wp == 1 && a.X == NN)))
+            // wp 1: the wave-function arrays' passes (X = N), wp 2: every strided
+            // pass; wp 3 / 4: as wp 1 with two warps per pencil pair in the z drift
+            // pass / in every wave-function pass (N = 512)
+            if (a.plan == 0 && (tu.wp == 2 || (tu.wp != 0 && a.X == NN))) {
+                if constexpr (NN == 512 && DF && (OP == OP_FWD || OP == OP_INV || OP == OP_DRIFT)) {
+                    if (tu.wp == 4 || (tu.wp == 3 && OP == OP_DRIFT))
+                        return launch_wp<NN, R, OP, DF, 2>(a, NZ, outer, pencil_dim, la3d, col0_ext, st);
+                }
                 return launch_wp<NN, R, OP, DF>(a, NZ, outer, pencil_dim, la3d, col0_ext, st);
+            }
         }
         if constexpr (strided_plan1<NN>()) {
             if (a.plan == 1) return launch_tma_e<NN, R, OP, PW, DF, 8, 1>(a, NZ, outer, pencil_dim, la3d, col0_ext, tu, st);

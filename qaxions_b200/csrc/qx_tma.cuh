@@ -466,22 +466,27 @@ __global__ void __launch_bounds__((tma_block_threads<N, R, PW, TXF>()), (tma_blo
 // stores to the tensor copy use the identity rows.
 // ---------------------------------------------------------------------------
 
+// barrier over the WPP warps that share pencil pair c (named barrier 1 + c)
+template <int WPP> __device__ __forceinline__ void pair_sync(int c) {
+    if constexpr (WPP == 1) __syncwarp();
+    else named_barrier(1 + c, 32 * WPP);
+}
 // a pencil pair's element p in the tensor copy's row p of a swizzled tile
-template <typename P> struct SwzRowAcc {
+template <typename P, int WPP = 1> struct SwzRowAcc {
     P* base;
     int c;
     __device__ __forceinline__ P& operator()(int p) const { return base[p * 8 + (c ^ (p & 7))]; }
-    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ void sync() const { pair_sync<WPP>(c); }
 };
 // the same slots with the exchange rows sigma(p)
-template <typename P> struct WarpXAcc {
+template <typename P, int WPP = 1> struct WarpXAcc {
     P* base;
     int c;
     __device__ __forceinline__ P& operator()(int p) const {
         const int r = p ^ ((p >> 3) & 7);
         return base[r * 8 + (c ^ (r & 7))];
     }
-    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ void sync() const { pair_sync<WPP>(c); }
 };
 
 constexpr int kWpTX = 16;        // tile columns
@@ -489,24 +494,34 @@ constexpr int kWpThreads = 256;  // 8 warps, one pencil pair each
 
 __host__ __device__ constexpr bool wp_supported(int N) { return N == 256 || N == 512; }
 
-// blockDim = (32, 8): lane t = threadIdx.x, pencil pair c = threadIdx.y
-template <int N, int OP, bool DF, int PLAN = 0>
-__global__ void __launch_bounds__(kWpThreads, 1) k_pencil_wp(const __grid_constant__ CUtensorMap tm, TArgs<float> s) {
+// WPP warps per pencil pair: WPP = 1 keeps E = N/32 values of each pencil per
+// lane (exchanges under __syncwarp); WPP = 2 (N = 512, the wave-function
+// passes) splits a pair over two warps with E = N/64, halving the registers so
+// that 16 warps fit on an SM, and synchronises the pair's exchanges with a
+// 64-thread named barrier.  The exchange rows are the same; with 64 threads
+// and radix-8 stages every exchange stays conflict-free (each 8-lane phase of
+// an access meets 8 distinct rows mod 8 after sigma).
+// blockDim = (32 WPP, 8): thread t = threadIdx.x of pencil pair c = threadIdx.y
+template <int N, int OP, bool DF, int PLAN = 0, int WPP = 1>
+__global__ void __launch_bounds__(kWpThreads * WPP, 1) k_pencil_wp(const __grid_constant__ CUtensorMap tm, TArgs<float> s) {
     using R = float;
     using C = float2;
     using P = CPair<C>;
     static_assert(wp_supported(N), "warp-per-pencil passes are compiled for N = 256, 512");
+    static_assert(WPP == 1 || (WPP == 2 && N == 512 && (OP == OP_FWD || OP == OP_INV || OP == OP_DRIFT)),
+                  "two warps per pencil pair: N = 512 wave-function passes only");
     constexpr int NL = qx_with_plan(N, PLAN);
-    constexpr int E = N / 32;
-    static_assert(E % qx_lcm_radices(NL) == 0, "N/32 values per lane must hold whole butterflies");
+    constexpr int TPP = 32 * WPP;
+    constexpr int E = N / TPP;
+    static_assert(E % qx_lcm_radices(NL) == 0, "values per thread must hold whole butterflies");
     constexpr int TX = kWpTX;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar[8];
     __shared__ int s_abort;
     __shared__ double red[32];
     const int t = threadIdx.x, c = threadIdx.y;
-    const int tid = threadIdx.x + 32 * threadIdx.y;
-    const int nthr = kWpThreads;
+    const int tid = threadIdx.x + TPP * threadIdx.y;
+    const int nthr = kWpThreads * WPP;
     const uint32_t tile_bytes = (uint32_t)((size_t)N * TX * sizeof(C));
     const long tile_elems = (long)(align1k(tile_bytes) / sizeof(C));
     C* bufs = reinterpret_cast<C*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -568,8 +583,8 @@ __global__ void __launch_bounds__(kWpThreads, 1) k_pencil_wp(const __grid_consta
         const int x0 = (int)(id % s.tiles_x) * TX;
         const int o = (int)(id / s.tiles_x);
         const int xb = x0 + 2 * c;
-        SwzRowAcc<P> io{reinterpret_cast<P*>(tile), c};
-        WarpXAcc<P> acc{reinterpret_cast<P*>(tile), c};
+        SwzRowAcc<P, WPP> io{reinterpret_cast<P*>(tile), c};
+        WarpXAcc<P, WPP> acc{reinterpret_cast<P*>(tile), c};
         const long id_next = id + gridDim.x;
         const bool a_copy = OP == OP_DRIFT && tid < TX && id_next < s.n_tiles;
         if (a_copy) {
@@ -664,8 +679,8 @@ __global__ void __launch_bounds__(kWpThreads, 1) k_pencil_wp(const __grid_consta
 
         if (a_copy) cp_async_wait_all();
         if (store) {
-            // the warp's finished pencil pair -> its slots (identity rows) -> tensor store
-            __syncwarp();
+            // the finished pencil pair -> its slots (identity rows) -> tensor store
+            pair_sync<WPP>(c);
             if constexpr (OP == OP_FWD) {
 #pragma unroll
                 for (int e = 0; e < E; ++e) io(out_pos<NL, E>(e, t)) = v[e];

@@ -56,3 +56,17 @@ def test_pencil_warp_against_fp64_oracle():
         f.psi = psi0
         f.step(n)
         assert O.rel_l2(f.psi, ref) < 1e-5
+
+
+@pytest.mark.parametrize("wp", [3, 4])
+@pytest.mark.parametrize("dim,N,steps", [(3, 512, 2), (2, 512, 6)])
+def test_two_warps_per_pencil_pair_bitwise(dim, N, steps, wp):
+    """wp 3 / 4: the drift pass / every wave-function pass with a pencil pair
+    split over two warps (8 values of each pencil per thread, pair barriers):
+    the same butterflies on the same operands, so bit for bit the one-warp
+    passes."""
+    a = _run(dim, N, 1, steps)
+    b = _run(dim, N, wp, steps)
+    for x, y in zip(a[:3], b[:3]):
+        assert np.array_equal(x, y)
+    assert a[3] == b[3]
