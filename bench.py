@@ -322,24 +322,27 @@ def run_ensemble(args, world, rank, local):
     dt = 0.2 / 128**2
     K, W = args.steps, args.warmup
     res = {}
-    for dtype in ("c64", "c128"):
-        e = qx.Ensemble(groups, dtype=dtype, dt=dt)
-        e.ic_config(qx.IC_GRF, seeds=seeds)
-        e.step(W)
-        barrier_sync(world)
-        ms = e.time_steps(K)
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        sites = torch.tensor([float(e.sites)], dtype=torch.float64, device=f"cuda:{local}")
-        if world > 1:
-            import torch.distributed as dist
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dist.all_reduce(sites, op=dist.ReduceOp.SUM)
-        res[dtype] = (float(t.item()), float(sites.item()))
-        e.close()
+    # mixed: one persistent launch per pass over the boxes of all sizes (work
+    # queue); per_size: one launch per pass per size, sizes on graph branches
+    for mixed in (True, "passes", False):
+        for dtype in ("c64", "c128"):
+            e = qx.Ensemble(groups, dtype=dtype, dt=dt, mixed=mixed)
+            e.ic_config(qx.IC_GRF, seeds=seeds)
+            e.step(W)
+            barrier_sync(world)
+            ms = e.time_steps(K)
+            t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+            sites = torch.tensor([float(e.sites)], dtype=torch.float64, device=f"cuda:{local}")
+            if world > 1:
+                import torch.distributed as dist
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                dist.all_reduce(sites, op=dist.ReduceOp.SUM)
+            res[(mixed, dtype)] = (float(t.item()), float(sites.item()))
+            e.close()
     acc = None
     if rank == 0 and args.accuracy_steps > 0:
-        a = qx.Ensemble(groups, dtype="c128", dt=dt)
-        b = qx.Ensemble(groups, dtype="c64", dt=dt)
+        a = qx.Ensemble(groups, dtype="c128", dt=dt, mixed=True)
+        b = qx.Ensemble(groups, dtype="c64", dt=dt, mixed=True)
         a.ic_config(qx.IC_GRF, seeds=seeds)
         b.ic_config(qx.IC_GRF, seeds=seeds)
         a.step(args.accuracy_steps)
@@ -352,8 +355,12 @@ def run_ensemble(args, world, rank, local):
         a.close()
         b.close()
     if rank == 0:
-        ms32, sites = res["c64"]
-        ms64, _ = res["c128"]
+        ms32, sites = res[("passes", "c64")]
+        ms64, _ = res[("passes", "c128")]
+        ps32, _ = res[(False, "c64")]
+        ps64, _ = res[(False, "c128")]
+        st32, _ = res[(True, "c64")]
+        st64, _ = res[(True, "c128")]
         value = sites * K / (ms32 / 1e3)
         print(json.dumps({
             "metric": "site-updates/s (ensemble 16x64^3 + 16x96^3 + 16x128^3, fused FP32 KDK)",
@@ -362,8 +369,17 @@ def run_ensemble(args, world, rank, local):
             "data": "synthetic",
             "config": {"workload": "ensemble of 48 GRF boxes (16x64^3, 16x96^3, 16x128^3), seeds 1234+b",
                        "sites": sites, "parallelism": f"instance sharding x{world}",
+                       "passes": "one persistent launch per pass over the boxes of all sizes, driven by a work "
+                                 "queue of (box, tile) units, costliest sizes first",
                        "l2": "state 415 MB complex64, larger than L2"},
             "plain_fp64": {"value": sites * K / (ms64 / 1e3), "ms_per_step": ms64 / K},
+            "launch_per_step": {"value": sites * K / (st32 / 1e3), "ms_per_step": st32 / K,
+                                "plain_fp64_value": sites * K / (st64 / 1e3), "plain_fp64_ms_per_step": st64 / K,
+                                "what": "the loop body of every box as ONE persistent launch per step: a queue of "
+                                        "(pass, box, tile) units, a unit waiting only for its box's previous pass"},
+            "per_size_launches": {"value": sites * K / (ps32 / 1e3), "ms_per_step": ps32 / K,
+                                  "plain_fp64_value": sites * K / (ps64 / 1e3), "plain_fp64_ms_per_step": ps64 / K,
+                                  "what": "one launch per pass per size, the sizes on concurrent graph branches"},
             "accuracy": acc}), flush=True)
 
 

@@ -273,6 +273,24 @@ int qx_ens_step(qx_ens_t *h, int nsteps);
 int qx_ens_time_steps(qx_ens_t *h, int nsteps, float *ms);
 /* mass sum |psi|^2 dV of every box (nboxes doubles) */
 int qx_ens_mass(qx_ens_t *h, double *M);
+/* Loop-body mode of the steps in between the first and the last of a call.
+ * mixed = 0 (default): each group's body replayed on its own stream (a graph
+ * branch per group, one launch per pass per group).  mixed = 1: the whole
+ * loop body of every box as ONE persistent launch per step, driven by a work
+ * queue of (pass, box, tile-or-rows) units (pass by pass, the costliest sizes
+ * first); a unit starts once its box has finished the previous pass, so the
+ * passes of different boxes overlap.  mixed = 2: one persistent launch per
+ * pass over the boxes of every size (the same queue, one pass at a time).
+ * Modes 1 and 2: 3D, STATIC cosmology, at most 4 groups, every N in
+ * {16, 32, 64, 96, 128} (QX_ERR_INVALID otherwise).  Every mode advances each
+ * box as its single-box run does. */
+int qx_ens_set_mixed(qx_ens_t *h, int mixed);
+/* Mode 1's queue runs the passes of windows of boxes whose psi and half
+ * spectrum together take at most `bytes` (at least one box per window) before
+ * moving to the next window, so a box's arrays can stay in the 126 MB L2 from
+ * one pass to the next.  0 = the default, 48 MiB; a value above the whole
+ * ensemble's size gives pass-by-pass order over all boxes. */
+int qx_ens_set_mixed_window(qx_ens_t *h, long long bytes);
 
 /* ---- learned corrector for coarse steps (no counterpart in the reference) ----
  * A periodic 3^3 convolutional network (4 -> 32 -> 32 -> 2 channels, GELU,

@@ -117,6 +117,8 @@ _SIGS = {
     "qx_ens_step": ([_vp, _i], _i),
     "qx_ens_time_steps": ([_vp, _i, _fp], _i),
     "qx_ens_mass": ([_vp, _dp], _i),
+    "qx_ens_set_mixed": ([_vp, _i], _i),
+    "qx_ens_set_mixed_window": ([_vp, C.c_longlong], _i),
 }
 for _name, (_args, _res) in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -507,12 +509,17 @@ class Ensemble:
     ``groups`` is a list of (N, count): count boxes of N^dim sites each.  Boxes
     of one size share one batched device array, so each pass of a step is one
     persistent launch over all of their tiles; groups run concurrently, each
-    replaying its loop body from a CUDA graph.  Boxes are numbered group by
-    group; box b's initial condition is seeded with seed_base + b.
+    replaying its loop body from a CUDA graph.  With ``mixed=True`` (3D, at
+    most 4 sizes from 16, 32, 64, 96, 128) the loop body of every box is
+    instead ONE persistent launch per step, fed by a work queue of (pass, box,
+    tile) units in which a unit starts once its box has finished the previous
+    pass; ``mixed="passes"`` runs the same queue as one launch per pass.  Boxes
+    are numbered group by group; box b's initial condition is seeded with
+    seed_base + b.
     """
 
     def __init__(self, groups, dim: int = 3, L: float = 1.0, pref: float = 1.0, dtype: str = "c64",
-                 dt: float | None = None):
+                 dt: float | None = None, mixed: bool = False):
         ns = [int(n) for n, _ in groups]
         cs = [int(c) for _, c in groups]
         if dt is None:
@@ -531,6 +538,24 @@ class Ensemble:
         _ens_check(_lib.qx_ens_size(self._h, C.byref(n), C.byref(sites)), self._h)
         self.nboxes = n.value
         self.sites = sites.value
+        self.mixed = False
+        if mixed:
+            self.set_mixed(mixed)
+
+    def set_mixed(self, mode=True):
+        """Loop bodies as one launch per step over all sizes (True), one launch
+        per pass over all sizes ("passes") or per-size launches on concurrent
+        graph branches (False); every mode advances each box as its
+        single-box run does."""
+        code = 2 if mode == "passes" else (1 if mode else 0)
+        self._c("qx_ens_set_mixed", code)
+        self.mixed = mode if code else False
+
+    def set_mixed_window(self, nbytes: int = 0):
+        """Bytes of boxes (psi + half spectrum) whose passes the one-launch
+        step runs together before the next window (0: default 48 MiB; more
+        than the ensemble: pass-by-pass order)."""
+        self._c("qx_ens_set_mixed_window", int(nbytes))
 
     def close(self):
         if getattr(self, "_h", None):

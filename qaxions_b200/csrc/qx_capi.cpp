@@ -464,8 +464,20 @@ struct qx_ens_s {
     std::vector<double> exec_dt;  // each group's ds when captured
     std::vector<cudaEvent_t> ev;  // per group: fork/join events
     cudaEvent_t ev0 = nullptr;
+    // mixed-size modes: 1 = the loop body as one persistent launch over every
+    // group, 2 = one launch per pass over every group.  Device counters: one
+    // queue counter per pass, then the one-launch body's per-(pass, box)
+    // completion counters, then its time-out flag
+    int dtype = QX_C128;
+    int mixed = 0;
+    unsigned long long* ctr = nullptr;
+    unsigned* done = nullptr;
+    int* dflag = nullptr;
+    size_t ctr_bytes = 0;
+    long long mix_window = 48LL << 20;  // bytes of boxes whose passes run together (mode 1)  // bytes cleared before every body (all but the flag)
     ~qx_ens_s() {
         if (exec) cudaGraphExecDestroy(exec);
+        if (ctr) cudaFree(ctr);
         for (auto e : ev) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (s0) cudaStreamDestroy(s0);
@@ -527,6 +539,7 @@ int qx_ens_create(int ngroups, const int* N, const int* boxes, int dim, double L
     const int rc = ens_guarded(h, [&](qx_ens_s& e) {
         need(ngroups > 0 && N && boxes, "need at least one group");
         need(dtype == QX_C128 || dtype == QX_C64, "dtype must be QX_C128 or QX_C64");
+        e.dtype = dtype;
         for (int g = 0; g < ngroups; ++g) {
             need(boxes[g] > 0, "every group needs at least one box");
             qx::FieldConfig c;
@@ -639,17 +652,70 @@ void ens_fork(qx_ens_s& e) {
     for (auto& g : e.groups) QX_CU(cudaStreamWaitEvent(g->stream(), e.ev0, 0));
 }
 
+// the loop body of every group on s0 with the mixed-size kernels: counters
+// cleared, then one launch (mode 1) or one launch per pass (mode 2)
+void ens_enqueue_mixed(qx_ens_s& e, const std::vector<qx::MixDesc>& d) {
+    QX_CU(cudaMemsetAsync(e.ctr, 0, e.ctr_bytes, e.s0));
+    const int ng = (int)d.size();
+    if (e.mixed == 1) {
+        if (e.dtype == QX_C64) qx::Mixed<float>::launch_step(d.data(), ng, e.ctr, e.done, e.dflag, (long)e.mix_window, e.s0);
+        else qx::Mixed<double>::launch_step(d.data(), ng, e.ctr, e.done, e.dflag, (long)e.mix_window, e.s0);
+        return;
+    }
+    for (int op = 0; op < qx::MX_NOPS; ++op) {
+        if (e.dtype == QX_C64) qx::Mixed<float>::launch(op, d.data(), ng, e.ctr + op, e.dflag, e.s0);
+        else qx::Mixed<double>::launch(op, d.data(), ng, e.ctr + op, e.dflag, e.s0);
+    }
+}
+
+void ens_alloc_counters(qx_ens_s& e) {
+    if (e.ctr) return;
+    const size_t nbox = e.group_of.size();
+    e.ctr_bytes = sizeof(unsigned long long) * qx::MX_NOPS + sizeof(unsigned) * qx::MX_NOPS * nbox;
+    void* p = nullptr;
+    QX_CU(cudaMalloc(&p, e.ctr_bytes + sizeof(int)));
+    e.ctr = static_cast<unsigned long long*>(p);
+    e.done = reinterpret_cast<unsigned*>(e.ctr + qx::MX_NOPS);
+    e.dflag = reinterpret_cast<int*>(static_cast<char*>(p) + e.ctr_bytes);
+    QX_CU(cudaMemset(p, 0, e.ctr_bytes + sizeof(int)));
+}
+
+// a time-out inside the one-launch body (a wait that gave up) -> error
+void ens_check_flag(qx_ens_s& e) {
+    if (!e.dflag) return;
+    int f = 0;
+    QX_CU(cudaMemcpy(&f, e.dflag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) {
+        QX_CU(cudaMemset(e.dflag, 0, sizeof(int)));
+        throw std::runtime_error(f == 2 ? "mixed-size passes: the host's unit layout disagrees with the kernel's"
+                                        : "mixed-size step: a wait for a box's previous pass timed out");
+    }
+}
+
 void ens_capture(qx_ens_s& e) {
     if (e.exec) cudaGraphExecDestroy(e.exec);
     e.exec = nullptr;
     for (auto& g : e.groups) g->prepare_replay();
     for (auto& g : e.groups) g->sync();
+    std::vector<qx::MixDesc> d;
+    if (e.mixed) {
+        ens_alloc_counters(e);
+        d.resize(e.groups.size());
+        for (size_t i = 0; i < e.groups.size(); ++i) e.groups[i]->mix_desc(d[i]);
+        // kernel attributes are set outside the capture
+        if (e.dtype == QX_C64) qx::Mixed<float>::prepare(d.data(), (int)d.size());
+        else qx::Mixed<double>::prepare(d.data(), (int)d.size());
+    }
     cudaGraph_t graph = nullptr;
     QX_CU(cudaStreamBeginCapture(e.s0, cudaStreamCaptureModeThreadLocal));
     try {
-        ens_fork(e);  // the group streams join the capture
-        for (auto& g : e.groups) g->enqueue_body(false);
-        ens_join(e);
+        if (e.mixed) {
+            ens_enqueue_mixed(e, d);
+        } else {
+            ens_fork(e);  // the group streams join the capture
+            for (auto& g : e.groups) g->enqueue_body(false);
+            ens_join(e);
+        }
     } catch (...) {
         cudaStreamEndCapture(e.s0, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -697,6 +763,7 @@ int qx_ens_step(qx_ens_t* h, int nsteps) {
         need(nsteps >= 0, "nsteps must be >= 0");
         ens_step(e, nsteps);
         for (auto& g : e.groups) g->sync();
+        ens_check_flag(e);
     });
 }
 
@@ -724,7 +791,41 @@ int qx_ens_time_steps(qx_ens_t* h, int nsteps, float* ms) {
         for (auto& ev : ends) cudaEventDestroy(ev);
         cudaEventDestroy(start);
         cudaEventDestroy(stop);
+        ens_check_flag(e);
         *ms = t;
+    });
+}
+
+int qx_ens_set_mixed(qx_ens_t* h, int mixed) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(mixed >= 0 && mixed <= 2, "mixed must be 0, 1 or 2");
+        if (mixed) {
+            need((int)e.groups.size() <= qx::kMixMaxGroups, "mixed-size passes take at most 4 groups");
+            for (auto& g : e.groups) {
+                need(g->dim() == 3, "mixed-size passes are 3D only");
+                need(g->cosmology() == 0, "mixed-size passes need the STATIC cosmology");
+                const bool ok = e.dtype == QX_C64 ? qx::Mixed<float>::supports(g->size())
+                                                  : qx::Mixed<double>::supports(g->size());
+                need(ok, ("mixed-size passes: grid size N=" + std::to_string(g->size()) + " is not compiled in").c_str());
+            }
+        }
+        if (mixed != e.mixed) {
+            if (e.exec) cudaGraphExecDestroy(e.exec);
+            e.exec = nullptr;
+            e.mixed = mixed;
+        }
+    });
+}
+
+int qx_ens_set_mixed_window(qx_ens_t* h, long long bytes) {
+    return ens_guarded(h, [&](qx_ens_s& e) {
+        need(bytes >= 0, "bytes must be >= 0");
+        const long long w = bytes ? bytes : (48LL << 20);
+        if (w != e.mix_window) {
+            if (e.exec) cudaGraphExecDestroy(e.exec);
+            e.exec = nullptr;
+            e.mix_window = w;
+        }
     });
 }
 

@@ -620,6 +620,24 @@ class FieldT final : public Field {
         vmax_stale_ = true;
     }
     void prepare_replay() override { ensure_axy(ds_); }
+    void mix_desc(MixDesc& d) override {
+        if (g_.dim != 3) throw std::invalid_argument("mixed-size passes are 3D only");
+        if (cosmo_ != 0) throw std::logic_error("mixed-size passes need the STATIC cosmology");
+        d.psi = psi();
+        d.vh = vh();
+        d.twN = tw_.N;
+        d.twN_lo = tw_.N_lo;
+        d.twM = tw_.M;
+        d.twNn = tw_.N_nat;
+        d.axy = ensure_axy(ds_);
+        d.N = g_.N;
+        d.B = g_.B;
+        d.pois_c = pois_c();
+        d.pois_g0 = pois_g0();
+        d.pref = pref_eff();
+        d.rho_mean = cfg_.rho_mean;
+        d.dt_kick = ds_;
+    }
 
     // Poisson source prefactor: pref (STATIC) or norm a with norm = 1 (MRE,
     // src/field.cxx:84-86,298)

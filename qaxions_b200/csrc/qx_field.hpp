@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "qx_mixed.hpp"
 #include "qx_ops.hpp"
 
 namespace qx {
@@ -166,6 +167,9 @@ class Field {
     virtual void enqueue_body(bool last) = 0;
     virtual void step_end(int nsteps) = 0;
     virtual void prepare_replay() = 0;
+    // the device arrays, tables and loop-body constants one pass launch over
+    // several fields of different sizes needs (3D; after prepare_replay)
+    virtual void mix_desc(MixDesc& d) = 0;
     // measure() (src/meas.cxx:13-63) without overwriting V (unless the mask
     // has MEAS_CLOBBER_V); files go to `dir` when it is not null
     virtual void measure(unsigned mask, int number, const char* dir, MeasRecord* rec) = 0;

@@ -179,12 +179,14 @@ def test_2d_256_500_steps_match_reference_build(dtype):
 
 
 @pytest.mark.parametrize("dtype", ["c128", "c64"])
-def test_96_cube_ensemble_box_matches_reference_build(dtype):
+@pytest.mark.parametrize("mixed", [False, True])
+def test_96_cube_ensemble_box_matches_reference_build(dtype, mixed):
     """A 96^3 box (radix 3) of a 3D ensemble (2 boxes of 64^3, 2 of 96^3 and
-    1 of 128^3 here) against the reference build stepping the same state."""
+    1 of 128^3 here) against the reference build stepping the same state, with
+    the per-size loop bodies and with one launch per pass over all sizes."""
     n = 20
     dt = 0.2 / 128**2
-    e = qx.Ensemble([(64, 2), (96, 2), (128, 1)], dtype=dtype, dt=dt)
+    e = qx.Ensemble([(64, 2), (96, 2), (128, 1)], dtype=dtype, dt=dt, mixed=mixed)
     e.ic_config(qx.IC_GRF, seed_base=77)
     box = 2  # the first 96^3 box
     assert e.box_n(box) == 96
@@ -200,7 +202,7 @@ def test_96_cube_ensemble_box_matches_reference_build(dtype):
     err = O.rel_l2(e.psi(box), ref.psi())
     ref.close()
     e.close()
-    _log({"test": "96_ensemble_box", "dtype": dtype, "relL2_psi": err})
+    _log({"test": "96_ensemble_box", "dtype": dtype, "mixed": mixed, "relL2_psi": err})
     assert err < (1e-12 if dtype == "c128" else 1e-5), err
 
 
