@@ -527,6 +527,206 @@ __global__ void __launch_bounds__(256) k_wgrad(const __nv_bfloat16* __restrict__
     if (tid < cout) outp[nw + tid] = bacc;
 }
 
+// Weight gradient on the tensor cores (tcgen05), the same sums as k_wgrad:
+//   dW[o][ci][co] = sum_s A[s + o][ci] dZ[s][co],  db[co] = sum_s dZ[s][co].
+// Per 8 x 8 x 4 brick (K = 256 sites) and per group of OPG = 128 / CINP
+// offsets, the block builds the group's shifted activations as the A operand
+// [128 rows (offset j, channel ci)] x [256 sites] in the canonical no-swizzle
+// K-major layout (core matrix (row group, 8-site chunk) at (rg * 32 + chunk) *
+// 128 B), and dZ of the brick once as the B operand [32 outputs] x [256 sites]
+// (BF16, the same layout); one thread issues 16 MMAs of M = 128, N = 32, K = 16
+// into the group's 32 tensor-memory columns, accumulating over every brick the
+// block processes.  Two group buffers alternate, so the next group is built
+// while the previous group's MMAs run; an mbarrier per buffer orders reuse.
+// dZ is rounded to BF16 for the tensor cores (the activations already are);
+// the bias gradient stays an FP32 sum.  Waits are bounded; tensor memory is
+// freed on every path.  partial: as k_wgrad.
+namespace wtc {
+constexpr int K = BSITES;            // 256 sites per brick
+constexpr int KCH = K / 8;           // 32 chunks of 8 sites
+constexpr int OPER_BYTES = 128 * K * 2;  // one A operand: 64 KB
+constexpr int DZ_BYTES = 32 * K * 2;     // B operand: 16 KB
+constexpr uint32_t LBO = 128, SBO = KCH * 128;
+template <int CINP> struct Geo {
+    static constexpr int OPG = 128 / CINP;                    // offsets per group
+    static constexpr int NGROUPS = (KOFF + OPG - 1) / OPG;    // 7 (CINP 32) or 4 (CINP 16)
+    static constexpr int HALO_BYTES = HALO * CINP * 2;
+    static constexpr size_t SMEM = 2 * (size_t)OPER_BYTES + DZ_BYTES + HALO_BYTES + 128;
+    static constexpr uint32_t TMEM_COLS = NGROUPS * 32 <= 128 ? 128 : 256;
+};
+}  // namespace wtc
+
+template <int CINP>
+__global__ void __launch_bounds__(256, 1) k_wgrad_tc(const __nv_bfloat16* __restrict__ A, const float* __restrict__ dZ,
+                                                     int N, int cin, int cout, float* partial, int* err) {
+    using G = wtc::Geo<CINP>;
+    constexpr int OPG = G::OPG, NG = G::NGROUPS;
+    using tc::commit;
+    using tc::fence_after;
+    using tc::fence_before;
+    using tc::mbar_init;
+    using tc::mbar_wait;
+    using tc::mma;
+    using tc::proxy_fence;
+    using tc::smem_addr;
+    using tc::smem_desc;
+    extern __shared__ __align__(128) unsigned char smem_w[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ float bred[8][32];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_w) + 127) & ~(uintptr_t)127);
+    unsigned char* oper[2] = {base, base + wtc::OPER_BYTES};
+    unsigned char* dzb = base + 2 * wtc::OPER_BYTES;
+    __nv_bfloat16* halo = reinterpret_cast<__nv_bfloat16*>(dzb + wtc::DZ_BYTES);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        mbar_init(smem_addr(&mbar[0]));
+        mbar_init(smem_addr(&mbar[1]));
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(G::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    const int nbx = N / BX, nby = N / BY, nbz = N / BZ;
+    const int nbricks = nbx * nby * nbz;
+    int ncommit[2] = {0, 0};  // commits issued on each buffer (the same in every thread)
+    int last = -1;            // buffer of the latest commit
+    float bsum = 0.f;         // bias partial of output tid % 32
+    bool first = true;
+    int fail = 0;             // this thread's wait timed out; combined at block barriers
+    auto wait_buf = [&](int b, long long limit) {
+        if (ncommit[b] > 0 && !mbar_wait(smem_addr(&mbar[b]), (uint32_t)((ncommit[b] - 1) & 1), limit)) fail = 1;
+    };
+    bool abort = false;
+    for (int br = blockIdx.x; br < nbricks && !abort; br += gridDim.x) {
+        const int bxi = br % nbx, byi = (br / nbx) % nby, bzi = br / (nbx * nby);
+        const int x0 = bxi * BX, y0 = byi * BY, z0 = bzi * BZ;
+        // the previous brick's MMAs read the halo, dZ and both buffers: wait for the last commit
+        if (last >= 0) wait_buf(last, 1LL << 31);
+        fence_after();
+        // periodic halo [hz][hy][hx][CINP] (16-byte copies)
+        for (int i = tid; i < HALO * (CINP / 8); i += blockDim.x) {
+            const int h = i / (CINP / 8), c = i % (CINP / 8);
+            const int hx = h % HX, hy = (h / HX) % HY, hz = h / (HX * HY);
+            const long gs = ((long)wrapi(z0 + hz - 1, N) * N + wrapi(y0 + hy - 1, N)) * N + wrapi(x0 + hx - 1, N);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(halo + (size_t)h * CINP + c * 8)),
+                         "l"(A + gs * CINP + c * 8)
+                         : "memory");
+        }
+        // dZ of the brick -> B operand: output co, chunk r = y + 8 z of 8 sites x = 0..7
+        for (int q = tid; q < 32 * wtc::KCH; q += blockDim.x) {
+            const int co = q % 32, r = q / 32;
+            const int y = r % BY, z = r / BY;
+            union {
+                __nv_bfloat162 h[4];
+                uint4 u;
+            } pk;
+#pragma unroll
+            for (int x2 = 0; x2 < 4; ++x2) {
+                float v0 = 0.f, v1 = 0.f;
+                if (co < cout) {
+                    const long g0 = ((long)(z0 + z) * N + (y0 + y)) * N + (x0 + 2 * x2);
+                    v0 = dZ[g0 * cout + co];
+                    v1 = dZ[(g0 + 1) * cout + co];
+                    bsum += v0 + v1;
+                }
+                pk.h[x2] = __floats2bfloat162_rn(v0, v1);
+            }
+            *reinterpret_cast<uint4*>(dzb + (size_t)((co / 8) * wtc::KCH + r) * 128 + (co % 8) * 16) = pk.u;
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if (__syncthreads_or(fail)) {
+            abort = true;
+            break;
+        }
+        for (int g = 0; g < NG; ++g) {
+            const int b = (ncommit[0] + ncommit[1]) & 1;
+            wait_buf(b, 1LL << 31);  // this buffer's previous MMAs are done
+            fence_after();
+            unsigned char* op = oper[b];
+            // rows m = j CINP + ci (offset o = g OPG + j), chunk r: the 8 sites
+            // x = 0..7 of row (y, z) shifted by the offset
+            for (int q = tid; q < 128 * wtc::KCH; q += blockDim.x) {
+                const int ci = q % CINP, rest = q / CINP;
+                const int r = rest % wtc::KCH, j = rest / wtc::KCH;
+                const int o = g * OPG + j;
+                const int y = r % BY, z = r / BY;
+                union {
+                    __nv_bfloat16 h[8];
+                    uint4 u;
+                } pk;
+                if (o < KOFF) {
+                    const int hb = (1 + off_dx(o)) + HX * ((1 + y + off_dy(o)) + HY * (1 + z + off_dz(o)));
+#pragma unroll
+                    for (int x = 0; x < 8; ++x) pk.h[x] = halo[(size_t)(hb + x) * CINP + ci];
+                } else {
+                    pk.u = make_uint4(0u, 0u, 0u, 0u);
+                }
+                const int m = j * CINP + ci;
+                *reinterpret_cast<uint4*>(op + (size_t)((m / 8) * wtc::KCH + r) * 128 + (m % 8) * 16) = pk.u;
+            }
+            proxy_fence();  // generic-proxy shared writes -> visible to the tensor cores
+            if (__syncthreads_or(fail)) {  // the same decision in every thread
+                abort = true;
+                break;
+            }
+            if (tid == 0) {
+                fence_after();
+                const uint32_t a0 = smem_addr(op), b0 = smem_addr(dzb);
+#pragma unroll 1
+                for (int kk = 0; kk < wtc::KCH / 2; ++kk)
+                    mma(tmem + (uint32_t)(g * 32), smem_desc(a0 + (uint32_t)(2 * kk * 128), wtc::LBO, wtc::SBO),
+                        smem_desc(b0 + (uint32_t)(2 * kk * 128), wtc::LBO, wtc::SBO), (!first || kk > 0) ? 1u : 0u);
+                commit(smem_addr(&mbar[b]));
+            }
+            ++ncommit[b];
+            last = b;
+        }
+        first = false;
+    }
+    // every MMA done before the accumulators are read (after a time-out: a
+    // longer bounded wait, so the MMAs in flight drain before tensor memory
+    // is freed)
+    if (last >= 0) wait_buf(last, abort ? (1LL << 32) : (1LL << 31));
+    if (last >= 0) wait_buf(last ^ 1, abort ? (1LL << 32) : (1LL << 31));
+    fence_after();
+    if (__syncthreads_or(fail)) abort = true;
+    const int nw = KOFF * cin * cout;
+    float* outp = partial + (long)blockIdx.x * (nw + cout);
+    if (!abort) {
+        // warp w reads lanes 32 (w % 4) .. of groups w / 4, w / 4 + 2, ...
+        for (int g = warp >> 2; g < NG; g += 2) {
+            float v[32];
+            tc::tmem_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(g * 32), v);
+            const int m = 32 * (warp & 3) + lane;
+            const int o = g * OPG + m / CINP, ci = m % CINP;
+            if (o < KOFF && ci < cin && !first) {
+                for (int co = 0; co < cout; ++co) outp[(o * cin + ci) * cout + co] = v[co];
+            } else if (o < KOFF && ci < cin) {  // no brick: zero partial
+                for (int co = 0; co < cout; ++co) outp[(o * cin + ci) * cout + co] = 0.f;
+            }
+        }
+    }
+    bred[warp][lane] = bsum;
+    fence_before();
+    __syncthreads();
+    if (tid < cout) {
+        float s = 0.f;
+        for (int w = 0; w < 8; ++w) s += bred[w][tid];
+        outp[nw + tid] = s;
+    }
+    if (abort && tid == 0) atomicExch(err, 1);
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::TMEM_COLS) : "memory");
+}
+
 // fixed-order fold of per-block partials: out[i] = sum_b partial[b][i] (FP64 sum)
 __global__ void k_fold(const float* partial, int nblk, int n, float* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -724,6 +924,10 @@ class Corrector {
         NN_CUDA(cudaMemset(errb_.p, 0, sizeof(int)));
         NN_CUDA(cudaFuncSetAttribute(k_wgrad<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgrad_smem(16, 32)));
         NN_CUDA(cudaFuncSetAttribute(k_wgrad<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgrad_smem(32, 32)));
+        NN_CUDA(cudaFuncSetAttribute(k_wgrad_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)wtc::Geo<32>::SMEM));
+        NN_CUDA(cudaFuncSetAttribute(k_wgrad_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)wtc::Geo<16>::SMEM));
     }
     ~Corrector() {
         if (st_) {
@@ -866,7 +1070,8 @@ class Corrector {
         NN_CUDA(cudaStreamSynchronize(st_));
         check_err();
     }
-    // 1: 32 -> 32 convolutions on the tcgen05 kernel (default), 0: all on mma.sync
+    // 1: 32-output convolutions and the weight gradients on the tcgen05 kernels
+    // (default), 0: convolutions on mma.sync, weight gradients on CUDA cores
     void set_tensor_path(int tc) { use_tc_ = tc != 0; }
     void check_err() {
         int e = 0;
@@ -934,10 +1139,16 @@ class Corrector {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const int nbricks = (int)(S_ / BSITES);
-        const int nblk = std::min(nbricks, 2 * sms);
         const int nw = KOFF * L.cin * L.cout;
+        // tensor cores (one block per SM, shared memory for two operand buffers),
+        // or the CUDA-core sums (set_tensor_path(0))
+        const int nblk = use_tc_ ? std::min(nbricks, sms) : std::min(nbricks, 2 * sms);
         part_.alloc(sizeof(float) * (size_t)nblk * (nw + L.cout));
-        k_wgrad<CINP><<<nblk, 256, wgrad_smem(CINP, L.cout), st_>>>(A, dZ, N_, L.cin, L.cout, part_.as<float>());
+        if (use_tc_)
+            k_wgrad_tc<CINP><<<nblk, 256, wtc::Geo<CINP>::SMEM, st_>>>(A, dZ, N_, L.cin, L.cout, part_.as<float>(),
+                                                                       errb_.as<int>());
+        else
+            k_wgrad<CINP><<<nblk, 256, wgrad_smem(CINP, L.cout), st_>>>(A, dZ, N_, L.cin, L.cout, part_.as<float>());
         fold_.alloc(sizeof(float) * (nw + L.cout));
         k_fold<<<(nw + L.cout + 255) / 256, 256, 0, st_>>>(part_.as<float>(), nblk, nw + L.cout, fold_.as<float>());
         NN_CUDA(cudaMemcpyAsync(L.gw.p, fold_.p, sizeof(float) * nw, cudaMemcpyDeviceToDevice, st_));

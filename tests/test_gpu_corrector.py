@@ -58,10 +58,12 @@ def test_corrector_gradients_match_cpu_oracle(tc):
 
 @pytest.mark.parametrize("N", [32, 96])
 def test_tensor_paths_agree(N):
-    """The tcgen05 kernel (8 x 16 x 2 bricks, tensor-memory accumulators) and the
-    mma.sync kernel compute the same 32 -> 32 convolutions: outputs and all
-    parameter gradients agree to FP32 summation order and the BF16 rounding of
-    the activations that follow (two calls each, so a stale state would show)."""
+    """The tcgen05 kernels (convolutions on 8 x 16 x 2 bricks; weight gradients
+    as im2col GEMMs; tensor-memory accumulators) and the mma.sync / CUDA-core
+    kernels compute the same network: outputs agree to FP32 summation order and
+    the BF16 rounding of the activations that follow, parameter gradients also
+    to the BF16 rounding of dZ that the tensor-core weight gradient takes (two
+    calls each, so a stale state would show)."""
     rng = np.random.default_rng(5 + N)
     psi_c = (1.0 + _smooth(rng, N, 0.3) + 1j * _smooth(rng, N, 0.2)).astype(np.complex64).astype(np.complex128)
     V = _smooth(rng, N, 2.0).astype(np.float32).astype(np.float64)
@@ -84,7 +86,7 @@ def test_tensor_paths_agree(N):
         assert np.isfinite(g1).all() and np.isfinite(y1).all()
         assert abs(l1 - l0) <= 1e-4 * l0, (l1, l0)
         assert O.rel_l2(y1, y0) <= 1e-3
-        assert O.rel_l2(g1, g0) <= 1e-3
+        assert O.rel_l2(g1, g0) <= 4e-3
     assert np.array_equal(res[True][0][1], res[True][1][1])  # deterministic
     for f in (fc, ff):
         f.close()
