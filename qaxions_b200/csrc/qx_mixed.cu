@@ -55,9 +55,12 @@ template <typename R> __host__ __device__ constexpr int mx_min_blocks() { return
 template <int N> __host__ __device__ constexpr int mx_e() { return qx_col_e(N); }
 template <int N> __host__ __device__ constexpr int mx_t() { return N / qx_col_e(N); }
 template <int N> __host__ __device__ constexpr int mx_slots() { return kUnitThreads / mx_t<N>(); }
-template <int N> __host__ __device__ constexpr int mx_pitch() {
-    return mx_slots<N>() * 16 < 128 ? mx_slots<N>() + 1 : mx_slots<N>();
-}
+// Unpadded: a warp's 8-lane phase of a 16-byte access covers 8 / S positions of
+// S slots each, and with S = 4 the two positions of a phase are consecutive
+// Stockham positions (an odd difference), so their 64-byte rows fall in
+// opposite halves of the 128-byte bank window; a padded pitch of S + 1 made
+// them overlap (ncu: 33 % of shared wavefronts were conflicts).
+template <int N> __host__ __device__ constexpr int mx_pitch() { return mx_slots<N>(); }
 // rows of an x-pass unit
 template <int N> __host__ __device__ constexpr int mx_rows() { return kUnitThreads / qx_row_threads(N); }
 
@@ -100,7 +103,7 @@ inline long mx_units_rt(int op, int N, int pw) {
 }
 inline int mx_unit_bytes_rt(int N, int csize) {
     const int S = kUnitThreads / (N / qx_col_e(N));
-    const int pitch = S * 16 < 128 ? S + 1 : S;
+    const int pitch = S;
     const int pencil = N * pitch * 16;
     const int rows = (kUnitThreads / qx_row_threads(N)) * row_smem_elems(N) * csize;
     return ((pencil > rows ? pencil : rows) + 15) & ~15;
