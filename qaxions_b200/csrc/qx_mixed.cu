@@ -520,8 +520,9 @@ __global__ void __launch_bounds__(kUnitThreads * kUnitsPerBlock, mx_min_blocks<R
 // The whole loop body as ONE persistent launch.  The queue lists the units of
 // pass 0 (every box), then pass 1, ... pass 7.  A unit of pass p > 0 of box b
 // starts once every unit of pass p - 1 of box b has finished (per-box
-// completion counters: release add after the unit's stores, acquire before
-// its loads), so the passes of different boxes overlap and no pass ends in a
+// completion counters: barrier, then one thread's release add after the
+// unit's stores; acquire before its loads), so the passes of different boxes
+// overlap and no pass ends in a
 // device-wide drain.  A unit only waits for units earlier in the queue, which
 // executors that are running have claimed and finish without waiting for any
 // later unit, so the launch always completes; every wait is bounded (~1 s of
@@ -624,14 +625,12 @@ __global__ void __launch_bounds__(kUnitThreads * kUnitsPerBlock, mx_min_blocks<R
             case MX_Y_INV_VH: mx_dispatch<R, MX_Y_INV_VH>(G, l, tu, bar, ubuf, tb); break;
             default: mx_dispatch<R, MX_X_C2R_KICK>(G, l, tu, bar, ubuf, tb); break;
         }
-        // publish: the unit's stores (ordered before thread 0 by the barrier)
-        // become visible GPU-wide before the counter moves (the grid-barrier
-        // pattern of cooperative groups: barrier, then one thread's fence)
+        // publish: the unit's stores are ordered before thread 0's release add
+        // by the barrier, and a release is cumulative, so a unit that acquires
+        // the counter sees them (a separate fence before the add measured 5 %
+        // slower: 1.827 against 1.743 ms per C4 step)
         unit_sync(bar);
-        if (tu == 0) {
-            __threadfence();
-            mx_red_release_add(a.done + (long)op * a.nbox + box, 1u);
-        }
+        if (tu == 0) mx_red_release_add(a.done + (long)op * a.nbox + box, 1u);
     }
 }
 
