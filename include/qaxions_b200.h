@@ -194,10 +194,17 @@ int qx_set_plan(qx_field_t *h, int plan);
  * agree to round-off. */
 int qx_set_pencil_warp(qx_field_t *h, int on);
 /* the launch geometry in use: out[10] = {x_rows, y_tx, la_tx, tma, nbuf, pw,
- * plan, chain, pencil_warp, from_cache}; from_cache = 1 when the field took it
- * from the autotuner's cache at creation (the process cache, or the file named
- * by the environment variable QX_TUNE_CACHE) */
+ * plan, chain, pencil_warp, from_cache}, and out[10] = row_stage when n >= 11;
+ * from_cache = 1 when the field took it from the autotuner's cache at creation
+ * (the process cache, or the file named by the environment variable
+ * QX_TUNE_CACHE) */
 int qx_get_tune(qx_field_t *h, int *out, int n);
+/* Row pass of the inverse x transform, density and r2c (the FP32 form, N >= 256;
+ * no counterpart in the reference, whose drift/updatePotential call library
+ * FFTs, src/field.cxx:119-198, 294-346): on = 1 copies each warp's next row
+ * into shared memory with cp.async while the current row is transformed, on = 0
+ * loads rows directly.  Bit-identical results. */
+int qx_set_row_stage(qx_field_t *h, int on);
 /* Drift chain (no counterpart in the reference: the reference's drift,
  * src/field.cxx:119-198, is three library FFT calls around a multiply).  on = 0
  * (default): the y forward, z drift and y inverse passes of a 3D complex64

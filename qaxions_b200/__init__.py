@@ -96,6 +96,7 @@ _SIGS = {
     "qx_set_chain": ([_vp, _i], _i),
     "qx_set_plan": ([_vp, _i], _i),
     "qx_set_pencil_warp": ([_vp, _i], _i),
+    "qx_set_row_stage": ([_vp, _i], _i),
     "qx_clear_tune_cache": ([], _i),
     "qx_get_tune": ([_vp, _ip, _i], _i),
     "qx_device_pointers": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], _i),
@@ -435,9 +436,10 @@ class Field:
     def get_tune(self) -> dict:
         """The launch geometry in use (and whether it came from the autotuner's
         cache when the field was created)."""
-        v = (C.c_int * 10)()
-        self._c("qx_get_tune", v, 10)
-        keys = ("x_rows", "y_tx", "la_tx", "tma", "nbuf", "pw", "plan", "chain", "pencil_warp", "from_cache")
+        v = (C.c_int * 11)()
+        self._c("qx_get_tune", v, 11)
+        keys = ("x_rows", "y_tx", "la_tx", "tma", "nbuf", "pw", "plan", "chain", "pencil_warp", "from_cache",
+                "row_stage")
         return dict(zip(keys, list(v)))
 
     def set_pencil_warp(self, on):
@@ -447,6 +449,12 @@ class Field:
         N = 512, 3 / 4 split each pencil pair over two warps in the drift pass /
         in every wave-function pass (bit for bit 1)."""
         self._c("qx_set_pencil_warp", int(on))
+
+    def set_row_stage(self, on):
+        """FP32 inverse x + density + r2c row pass (N >= 256): 1 copies each
+        warp's next row into shared memory with cp.async while the current one
+        is transformed, 0 loads rows directly (bit-identical)."""
+        self._c("qx_set_row_stage", int(on))
 
     def set_chain(self, on):
         """Drift chain: the y, z-drift, y passes of a 3D complex64 field as

@@ -304,9 +304,17 @@ int qx_get_tune(qx_field_t* h, int* out, int n) {
     return guarded(h, [&](qx::Field& f) {
         need(out && n >= 10, "out must hold 10 ints");
         const qx::Tune& t = f.tune();
-        const int v[10] = {t.x_rows, t.y_tx, t.la_tx, t.tma, t.nbuf, t.pw, t.plan, t.chain, t.wp,
-                           f.tuned_from_cache() ? 1 : 0};
-        for (int i = 0; i < 10; ++i) out[i] = v[i];
+        const int v[11] = {t.x_rows, t.y_tx, t.la_tx, t.tma, t.nbuf, t.pw, t.plan, t.chain, t.wp,
+                           f.tuned_from_cache() ? 1 : 0, t.xstage};
+        for (int i = 0; i < (n < 11 ? n : 11); ++i) out[i] = v[i];
+    });
+}
+
+int qx_set_row_stage(qx_field_t* h, int on) {
+    return guarded(h, [&](qx::Field& f) {
+        need(on == 0 || on == 1, "on must be 0 or 1");
+        f.tune().xstage = on;
+        f.invalidate_graph();
     });
 }
 

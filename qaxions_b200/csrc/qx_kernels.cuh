@@ -358,28 +358,60 @@ __device__ __forceinline__ void r2c_post_store(RowAcc<cx_t<R>>& acc, int t, cx_t
     }
 }
 
-enum XInvMode { XI_PLAIN = 0, XI_R2C = 1 };
+enum XInvMode { XI_PLAIN = 0, XI_R2C = 1, XI_STAGE = 2 };
 
-// inverse c2c along x (psi^_x -> psi, times scale); optionally the density
-// source pref(|psi|^2 - rho_mean) and its r2c x transform into vh.
+// staging buffer of an x inverse row pass with XI_STAGE (FP32): the next row (N)
+template <int N, typename R, int MODE> __host__ __device__ constexpr int x_inv_stage_elems() {
+    return (sizeof(R) == 4 && (MODE & XI_STAGE)) ? N : 0;
+}
+
+// inverse c2c along x (psi^_x -> psi, times scale); optionally (XI_R2C) the
+// density source pref(|psi|^2 - rho_mean) and its r2c x transform into vh.
+// XI_STAGE (FP32): software-pipelined like the kicking c2r pass -- once every
+// lane has read its row from the staging buffer, the warp copies its next row
+// there with cp.async, so that row arrives while the current one is transformed.
 template <int N, typename R, int MODE>
 __global__ void __launch_bounds__(256, 2) k_x_inv(XArgs<R> a) {
     using C = cx_t<R>;
     constexpr int E = qx_row_efull(N);
     constexpr int M = N / 2;
     constexpr int EH = E / 2;
+    constexpr int T = qx_row_threads(N);
     constexpr bool PAIRED = row_paired<N>();
+    constexpr int SE = x_inv_stage_elems<N, R, MODE>();
+    constexpr bool STAGE = SE > 0;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     XTabs<C> tb;
     C* sm = x_setup<N, R>(a, smem_raw, tb);
     const int t = threadIdx.x;
     RowAcc<C> acc{sm, warp_lanes_mask()};
+    C* stg = x_stage_ptr<N>(sm, SE);
+    auto prefetch = [&](long r) {
+        if constexpr (STAGE) {
+            const char* gp = reinterpret_cast<const char*>(a.in + r * N);
+            char* sp = reinterpret_cast<char*>(stg);
+            for (int i = t; i < (int)(N * sizeof(C) / 16); i += T) cp_async16(sp + 16 * i, gp + 16 * i);
+            cp_async_commit();
+        }
+    };
+    if (STAGE && x_row0() < a.rows) prefetch(x_row0());
     for (long row = x_row0(); row < a.rows; row += x_row_step()) {
         acc.sync();
-        const C* src = a.in + row * N;
         C v[E];
+        if constexpr (STAGE) {
+            cp_async_wait_all();
+            acc.sync();
 #pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = src[out_pos<N, E>(e, t)];
+            for (int e = 0; e < E; ++e) v[e] = stg[out_pos<N, E>(e, t)];
+            // every lane has its values: fetch the next row
+            acc.sync();
+            const long nrow = row + x_row_step();
+            if (nrow < a.rows) prefetch(nrow);
+        } else {
+            const C* src = a.in + row * N;
+#pragma unroll
+            for (int e = 0; e < E; ++e) v[e] = src[out_pos<N, E>(e, t)];
+        }
         ifft_pencil_rev<N, E, PAIRED ? 1 : 0>(v, acc, t, tw_src<true>(tb.N, tb.N_lo));
         const R sc = (R)a.scale;
         C* dst = a.out + row * N;
@@ -393,7 +425,7 @@ __global__ void __launch_bounds__(256, 2) k_x_inv(XArgs<R> a) {
 #pragma unroll
             for (int e = 0; e < E; ++e) dst[in_pos<N, E, 0>(e, t)] = v[e];
         }
-        if constexpr (MODE == XI_R2C) {
+        if constexpr ((MODE & XI_R2C) != 0) {
             const R pr = (R)a.pref, rm = (R)a.rho_mean;
             auto src_of = [&](const C& u) { return pr * (u.x * u.x + u.y * u.y - rm); };
             C z[EH];  // (rho[2q], rho[2q+1]), q = in_pos<M, EH, 0>(e, t)

@@ -32,6 +32,9 @@ struct Tune {
                       // (grids whose plan has radices of different sizes: 64, 96, 128, 256)
     int chain = 0;    // FP32 3D drift's y / z / y passes: 0 three passes; 1 / 2 one slab-ordered
                       // kernel over slabs of `chain` 8-column tiles (bit-identical, measured slower)
+    int xstage = 0;   // FP32 x inverse + density + r2c pass (N >= 256): 1 = each warp copies its
+                      // next row into shared memory with cp.async while it transforms the
+                      // current one; 0 = direct loads (bit-identical)
 };
 
 template <typename R> struct Ops {

@@ -141,6 +141,14 @@ void Ops<R>::x_inv(int N, const XP& a, bool r2c, const Tune& tu, cudaStream_t st
     const XArgs<R> x = to_x<R>(a);
     const int P = x_rows_per_block(N, a.rows, tu.x_rows);
     QX_FOR_N(N, {
+        if constexpr (sizeof(R) == 4 && NN >= 256) {
+            // software-pipelined density + r2c pass (tu.xstage)
+            if (r2c && tu.xstage == 1) {
+                launch_x<R, NN>(k_x_inv<NN, R, XI_R2C | XI_STAGE>, x, P, st,
+                                x_inv_stage_elems<NN, R, XI_R2C | XI_STAGE>());
+                return;
+            }
+        }
         if (r2c) launch_x<R, NN>(k_x_inv<NN, R, XI_R2C>, x, P, st);
         else launch_x<R, NN>(k_x_inv<NN, R, XI_PLAIN>, x, P, st);
     });

@@ -642,11 +642,11 @@ __global__ void __launch_bounds__(kWpThreads * WPP, 1) k_pencil_wp(const __grid_
 #pragma unroll
                     for (int e = 0; e < E; ++e) col0[out_pos<NL, E>(e, t)] = pen(v[e], 0);
                 } else if (has_col0 && !s.col0_external) {
-                    // 2D: the mirror -k_y of column 0 lies in the same pencil (this warp's)
-                    __syncwarp();
+                    // 2D: the mirror -k_y of column 0 lies in the same pencil (this pair's)
+                    pair_sync<WPP>(c);
 #pragma unroll
                     for (int e = 0; e < E; ++e) acc(out_pos<NL, E>(e, t)) = v[e];
-                    __syncwarp();
+                    pair_sync<WPP>(c);
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
                         const int p = out_pos<NL, E>(e, t);
@@ -670,8 +670,8 @@ __global__ void __launch_bounds__(kWpThreads * WPP, 1) k_pencil_wp(const __grid_
             }
             ifft_pencil_rev<NL, E>(v, acc, t, tw_src<DF>(tws, tws_lo));
             if (c0ext) {
-                // the stash was written by other lanes of this warp in another order;
-                // the inverse's exchanges synchronised the warp since
+                // the stash was written by other threads of this pencil pair in another
+                // order; the inverse's exchanges synchronised the pair since
 #pragma unroll
                 for (int e = 0; e < E; ++e) pen(v[e], 0) = col0[in_pos<NL, E, 0>(e, t)];
             }

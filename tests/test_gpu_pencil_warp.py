@@ -14,10 +14,12 @@ from oracle import sp_oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def _run(dim, N, wp, steps, seed=77):
+def _run(dim, N, wp, steps, seed=77, row_stage=0):
     f = qx.Field(dim, N, pref=1.0, dtype="c64", k0="reference", dt=0.2 / N**2)
     f.set_pencil_warp(wp)
+    f.set_row_stage(row_stage)
     assert f.get_tune()["pencil_warp"] == wp
+    assert f.get_tune()["row_stage"] == row_stage
     f.ic_config(qx.IC_GRF, seed, 4, 0.02, 0.05)
     f.step(steps)
     psi = f.psi
@@ -67,6 +69,18 @@ def test_two_warps_per_pencil_pair_bitwise(dim, N, steps, wp):
     passes."""
     a = _run(dim, N, 1, steps)
     b = _run(dim, N, wp, steps)
+    for x, y in zip(a[:3], b[:3]):
+        assert np.array_equal(x, y)
+    assert a[3] == b[3]
+
+
+@pytest.mark.parametrize("dim,N,steps", [(3, 512, 2), (3, 256, 3), (2, 512, 6)])
+def test_staged_row_pass_bitwise(dim, N, steps):
+    """Row stage 1: the inverse x + density + r2c pass reads each row from a
+    shared-memory copy made by cp.async one row ahead -- the same values in the
+    same registers, so bit for bit the direct-load pass."""
+    a = _run(dim, N, 3 if N == 512 else 1, steps, row_stage=0)
+    b = _run(dim, N, 3 if N == 512 else 1, steps, row_stage=1)
     for x, y in zip(a[:3], b[:3]):
         assert np.array_equal(x, y)
     assert a[3] == b[3]
