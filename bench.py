@@ -650,7 +650,8 @@ def main():
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": ms_step, "steps_per_s": 1e3 / ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
             "dtype": "c64 (fp32 complex; fp64 phase args, reductions, spectrum sums)", "data": "synthetic",
             "config": {"workload": "3D 512^3 GRF + 32 Schive solitons, merged KDK step (fused FP32 form)",
                        "grid": N_GRID, "dim": DIM, "dt": dt, "pref": 1.0, "seed": SEED,
@@ -662,7 +663,11 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": 5 + 8 * K,
+            # qx_step(K) in 3D: a prologue of 6 launches (x r2c, y fwd, z Poisson
+            # + its column-0 kernel, y inv, x c2r + half kick + x fwd), then K loop
+            # bodies of 9 (y fwd, z drift, y inv, x inv + r2c, y fwd, z Poisson,
+            # column 0, y inv, x c2r + kick + x fwd)
+            "gpu_launches": 6 + 9 * K,
             "clocks": clocks,
             "accuracy": acc,
         }
