@@ -156,7 +156,7 @@ def time_form(qx, dtype, dt, K, W, world, device, sample_clocks=False, autotune=
     if autotune:
         # the autotuner times each candidate launch geometry for a few steps and
         # keeps the fastest (state restored); later fields of this grid reuse it
-        t_ms, cached = f.autotune(2)
+        t_ms, cached = f.autotune(4)
         tune = dict(f.get_tune(), tuned_ms_per_step=t_ms)
     f.step(W)                     # warm-up (also captures the loop-body graph)
     barrier_sync(world)
