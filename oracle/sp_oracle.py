@@ -414,18 +414,22 @@ def add_schive_solitons(psi: np.ndarray, rc, phase, centres, L: float = 1.0,
     dim, N = psi.ndim, psi.shape[0]
     dx = L / N
     c = np.arange(N) * dx
-    if dim == 2:
-        Y, X = np.meshgrid(c, c, indexing="ij")
-        Z = None
-    else:
-        Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
     out = psi.astype(np.complex128).copy()
+
+    def mi(d):
+        return d - L * np.rint(d / L)
+
     for j in range(len(rc)):
-        def mi(d):
-            return d - L * np.rint(d / L)
-        r2 = mi(X - centres[j, 0] * L) ** 2 + mi(Y - centres[j, 1] * L) ** 2
-        if dim == 3:
-            r2 = r2 + mi(Z - centres[j, 2] * L) ** 2
+        # each axis' minimum-image term depends on that coordinate alone:
+        # 1D terms broadcast over the grid (the same values, summed in the
+        # same order, as full coordinate grids would give)
+        ax = mi(c - centres[j, 0] * L) ** 2
+        ay = mi(c - centres[j, 1] * L) ** 2
+        if dim == 2:
+            r2 = ax[None, :] + ay[:, None]
+        else:
+            az = mi(c - centres[j, 2] * L) ** 2
+            r2 = (ax[None, None, :] + ay[None, :, None]) + az[:, None, None]
         out += schive_amplitude(np.sqrt(r2), rc[j], rho0) * np.exp(1j * phase[j])
     return out
 
